@@ -1,0 +1,184 @@
+/*
+ * salgpu.h -- C ABI of the B200 SAL-gradient treecode (libsalgpu.so).
+ *
+ * Drop-in boundary for cygnari/sal-fort's fast-sum entry points.  The reference
+ * is Fortran; its callers bind these functions with ISO_C_BINDING (the
+ * interface block is in sal-fort_b200/fortran/salgpu_mod.f90).  Signatures use
+ * plain pointers and sizes only.
+ *
+ * Conventions
+ *   - Panel ids, point ids and interaction-list entries are 1-based, exactly as
+ *     the reference's Fortran arrays hold them (tree_module.f90:5-34).
+ *   - Point arrays (xs, ys, zs, areas, sshs, outputs) are 0-based C arrays of
+ *     point_count doubles in the caller's point order.
+ *   - Every function returns SAL_OK (0) or a negative SAL_E* code;
+ *     sal_last_error() gives the message of the last failure on this thread.
+ *   - Functions whose names end in _host take host pointers and are synchronous.
+ *     sal_solve and sal_direct_sum take device pointers and a cudaStream_t
+ *     (passed as void*) and are asynchronous on that stream.
+ *   - There is no CPU fallback: without a usable CUDA device every device entry
+ *     point returns SAL_ENODEV.
+ */
+#ifndef SALGPU_H
+#define SALGPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SAL_OK 0
+#define SAL_EINVAL (-1)
+#define SAL_ENOMEM (-2)
+#define SAL_ECUDA (-3)
+#define SAL_ETIMEOUT (-4)
+#define SAL_ENODEV (-5)
+
+/* Evaluator families.  DTT is the code.f90 path (fast_sum_module.f90); the two
+ * STT modes are the mom6_code.f90 path (mom6_fast_sum_module.f90). */
+#define SAL_MODE_DTT 0               /* dual tree traversal, PP/PC/CP/CC */
+#define SAL_MODE_STT_REF_COMPAT 1    /* single tree traversal, proxy weights stored transposed as the reference does */
+#define SAL_MODE_STT_CORRECT 2       /* single tree traversal, proxy weights in the orientation pc_interact reads */
+
+/* Arithmetic forms of a solve. */
+#define SAL_FORM_REF 0       /* FP64, the reference's kernel and interpolation operation for operation */
+#define SAL_FORM_ACCURATE 1  /* FP64; CP/CC interpolate the frame-free Cartesian sum and use the antipode-stable kernel */
+#define SAL_FORM_MIXED 2     /* ACCURATE's algorithm with FP32 kernel tiles and tensor-core contractions; FP64 self/near pairs */
+
+typedef struct sal_tree sal_tree;  /* host cubed-sphere quadtree (tree_module.f90 cube_panel array) */
+typedef struct sal_grid sal_grid;  /* device-resident grid: points, panels, lists, work plan */
+
+/* ------------------------------------------------------------------ errors */
+const char *sal_last_error(void);
+void sal_free(void *p);  /* frees arrays returned by the list builders below */
+
+/* ------------------------------------------------------------------ host setup
+ * These mirror tree_module.f90 for callers that build the tree in C/C++.  A
+ * Fortran caller keeps its own tree_traverse/dual_tree_traversal and passes the
+ * flattened result to sal_tree_import instead. */
+
+/* tree_traverse, tree_module.f90:59-246. */
+int sal_tree_traverse(const double *xs, const double *ys, const double *zs, int32_t point_count,
+                      int32_t cluster_thresh, sal_tree **out);
+
+/* Import a cube_panel array flattened by the caller (tree_module.f90:5-28)
+ * together with the points it was built from.
+ * ints9: per panel level, is_leaf, id, parent, child1..child4, face.
+ * dbl7:  per panel min_xi, mid_xi, max_xi, min_eta, mid_eta, max_eta, radius.
+ * pt_off (npanels+1) / pt_idx: CSR of points_inside (1-based point ids).
+ * Every leaf's points_inside together must be a partition of 1..point_count,
+ * and every panel's count must equal the sum of its children's. */
+int sal_tree_import(int32_t npanels, const int32_t *ints9, const double *dbl7, const int64_t *pt_off,
+                    const int32_t *pt_idx, int32_t point_count, const double *xs, const double *ys,
+                    const double *zs, sal_tree **out);
+
+/* Sizes of a tree: panel count, total length of all points_inside arrays, deepest level. */
+int sal_tree_info(const sal_tree *t, int32_t *npanels, int64_t *points_inside_total, int32_t *max_level);
+
+/* Export in the sal_tree_import layout (pt_idx may be NULL). */
+int sal_tree_export(const sal_tree *t, int32_t *ints9, double *dbl7, int64_t *pt_off, int32_t *pt_idx);
+
+int sal_tree_destroy(sal_tree *t);
+
+/* dual_tree_traversal, tree_module.f90:277-398.  *list receives count triplets
+ * (index_target, index_source, interact_type 0..3); free with sal_free. */
+int sal_dual_tree_traversal(const sal_tree *t, double theta, int32_t cluster_thresh, int32_t **list,
+                            int64_t *count);
+
+/* single_tree_traversal, tree_module.f90:401-487.  *pc and *pp receive pairs
+ * (index_target = point id, index_source = panel id); free with sal_free. */
+int sal_single_tree_traversal(const sal_tree *t, double theta, int32_t cluster_thresh, const double *xs,
+                              const double *ys, const double *zs, int32_t own_points, int32_t **pc,
+                              int64_t *npc, int32_t **pp, int64_t *npp);
+
+/* assign_points_to_panels, tree_module.f90:249-273.  points_panels is
+ * (nlev x own_points) column-major and is filled with -1 first. */
+int sal_assign_points_to_panels(const sal_tree *t, const double *xs, const double *ys, const double *zs,
+                                int32_t own_points, int32_t *points_panels, int32_t nlev);
+
+/* ------------------------------------------------------------------ device grid */
+typedef struct {
+    int32_t point_count;
+    const double *xs, *ys, *zs, *areas;  /* host, caller's order */
+    int32_t interp_degree;               /* namelist interp_degree (code.f90:14) */
+    int32_t mode;                        /* SAL_MODE_* */
+    /* DTT: list_count triplets (target panel, source panel, type). */
+    const int32_t *list;
+    int64_t list_count;
+    /* STT: pairs (target point, source panel). */
+    const int32_t *pc_list;
+    int64_t pc_count;
+    const int32_t *pp_list;
+    int64_t pp_count;
+    int32_t max_fields;  /* largest number of SSH fields one sal_solve call may carry (>= 1) */
+    int32_t device;      /* CUDA device ordinal */
+} sal_grid_desc;
+
+typedef struct {
+    int32_t point_count, npanels, nleaves, degree, mode;
+    int64_t list_count;
+    double pairs_pp, pairs_pc, pairs_cp, pairs_cc;  /* kernel evaluations per field per solve */
+    double macs_up, macs_down;                       /* proxy multiply-adds per field per solve */
+    int64_t device_bytes;                            /* resident device memory of the grid */
+    double setup_seconds;                            /* plan build + upload */
+} sal_grid_stats;
+
+/* Flattens the tree and lists into device-resident arrays (once per grid). */
+int sal_grid_create(const sal_tree *t, const sal_grid_desc *desc, sal_grid **out);
+int sal_grid_stats_get(const sal_grid *g, sal_grid_stats *s);
+
+/* Waits for the grid's work on stream (NULL: the grid's own stream) and
+ * returns SAL_ETIMEOUT if a device-side staging wait gave up since the last
+ * check. */
+int sal_grid_sync(sal_grid *g, void *stream);
+
+/* Per-pass device timers.  enable = 1 turns them on (each FP64 solve then
+ * records CUDA events on its stream around three passes and waits for the
+ * last), 0 turns them off, -1 leaves them as they are; 1 and 0 also reset the
+ * sums.  phase_ms (4 doubles, may be NULL) receives the summed milliseconds of
+ * prep+upward, proxy potentials, leaf evaluation and their total; solves the
+ * number of solves summed. */
+int sal_grid_timing(sal_grid *g, int32_t enable, double *phase_ms, int64_t *solves);
+
+/* Throughput of the FP64 (precision 64) or FP32 (precision 32) fused
+ * multiply-add pipe of the current device, measured by a dependent-chain
+ * microbenchmark: *tflops receives the achieved TFLOP/s (2 flops per FMA). */
+int sal_fma_peak(int32_t precision, double *tflops);
+int sal_grid_destroy(sal_grid *g);
+
+/* Batched solve on device buffers.  ssh: nfields columns of point_count
+ * doubles, column f at ssh + f*ld_ssh, caller's point order.  Outputs likewise
+ * (overwritten, not accumulated).  form is SAL_FORM_*; SAL_FORM_REF supports
+ * nfields == 1 per column loop.  Asynchronous on stream. */
+int sal_solve(sal_grid *g, const double *ssh, int32_t nfields, int64_t ld_ssh, double *out_x, double *out_y,
+              int64_t ld_out, int32_t form, void *stream);
+
+/* fast_sum, fast_sum_module.f90:291-332: adds the SAL gradient of one field
+ * into host arrays sal_longrad/sal_latgrad (intent(inout)).  The grid must be
+ * SAL_MODE_DTT.  form as in sal_solve. */
+int sal_fast_sum_host(sal_grid *g, const double *ssh, double *sal_longrad, double *sal_latgrad, int32_t form);
+
+/* proxy_source_compute, mom6_fast_sum_module.f90:33-74: adds the proxy source
+ * weights of every panel into proxy_source_weights ((d+1)^2 * npanels,
+ * panel-major, the reference's flat layout; transposed in
+ * SAL_MODE_STT_REF_COMPAT). */
+int sal_proxy_source_compute_host(sal_grid *g, const double *sshs, double *proxy_source_weights);
+
+/* pc_compute, mom6_fast_sum_module.f90:153-174: adds the far field computed
+ * from proxy_weights (as returned above, possibly summed across ranks). */
+int sal_pc_compute_host(sal_grid *g, const double *proxy_weights, double *sal_x, double *sal_y);
+
+/* pp_compute, mom6_fast_sum_module.f90:177-192 (one rank, no halo points). */
+int sal_pp_compute_host(sal_grid *g, const double *sshs, double *sal_x, double *sal_y);
+
+/* FP64 direct O(N^2) sum at nt targets (0-based indices into the sources),
+ * with the reference kernel in its own operation order.  Device pointers;
+ * w = area * ssh per source.  Overwrites out_x/out_y (nt each). */
+int sal_direct_sum(const double *xs, const double *ys, const double *zs, const double *w, int32_t n,
+                   const int32_t *targets, int32_t nt, double *out_x, double *out_y, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SALGPU_H */

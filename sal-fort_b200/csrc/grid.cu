@@ -1,0 +1,495 @@
+// Device-resident grids and the solve entry points of the C ABI.
+#include <cuda_runtime.h>
+
+#include <chrono>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/salgpu.h"
+#include "kernels.cuh"
+#include "sal_internal.hpp"
+
+namespace sal {
+int set_error(int code, const std::string &msg);  // capi.cpp
+}
+
+using namespace sal;
+
+namespace {
+
+template <class T>
+struct DBuf {
+    T *p = nullptr;
+    size_t n = 0;
+};
+
+struct GridImpl {
+    int dev = 0;
+    Plan plan;
+    cudaStream_t stream = nullptr;
+    int64_t bytes = 0;
+    double setup_seconds = 0;
+    int nsrc = 0, ntgt = 0, rec_stride = 0, nup = 0, nproxy_units = 0;
+    // device arrays
+    double4 *xyz = nullptr;       // pool order x, y, z (w unused)
+    double *area = nullptr;
+    double2 *xieta = nullptr;
+    int32_t *perm = nullptr;
+    double4 *pool = nullptr;      // n points + nsrc*P proxies
+    Group *leaf_groups = nullptr;
+    Item *leaf_items = nullptr;
+    uint32_t *masks = nullptr;
+    Group *proxy_groups = nullptr;
+    Item *proxy_items = nullptr;
+    int32_t *proxy_unit_beg = nullptr;
+    double4 *tgt_proxy = nullptr;
+    double *records = nullptr;
+    double4 *proxy_partial = nullptr;
+    UpUnit *up_units = nullptr;
+    int32_t *up_unit_beg = nullptr;
+    double *src_nodes = nullptr;
+    double *up_partial = nullptr;
+    int *err = nullptr;
+    // staging for the *_host entry points
+    double *h_ssh = nullptr, *h_ox = nullptr, *h_oy = nullptr;  // device
+    double *h_w = nullptr;                                        // device, P*npanels
+    std::vector<void *> allocs;
+    std::mutex mu;
+    // optional per-pass timers: events recorded on the launching stream
+    bool timing = false;
+    cudaEvent_t ev[8] = {};
+    double phase_ms[4] = {0, 0, 0, 0};   // prep+upward, proxy, leaf, total
+    int64_t phase_solves = 0;
+};
+
+}  // namespace
+
+struct sal_grid {
+    GridImpl g;
+};
+struct sal_tree : sal::Tree {};
+
+#define CK(call)                                                                                  \
+    do {                                                                                          \
+        cudaError_t e_ = (call);                                                                  \
+        if (e_ != cudaSuccess)                                                                    \
+            return set_error(SAL_ECUDA, std::string(#call) + ": " + cudaGetErrorString(e_));     \
+    } while (0)
+
+template <class T>
+static int dalloc(GridImpl &g, T **p, size_t count) {
+    *p = nullptr;
+    if (count == 0) return SAL_OK;
+    cudaError_t e = cudaMalloc((void **)p, count * sizeof(T));
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        return set_error(e == cudaErrorMemoryAllocation ? SAL_ENOMEM : SAL_ECUDA,
+                         std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    }
+    g.allocs.push_back(*p);
+    g.bytes += (int64_t)(count * sizeof(T));
+    return SAL_OK;
+}
+
+template <class T>
+static int dupload(GridImpl &g, T **p, const T *src, size_t count) {
+    int rc = dalloc(g, p, count);
+    if (rc) return rc;
+    if (count) CK(cudaMemcpy(*p, src, count * sizeof(T), cudaMemcpyHostToDevice));
+    return SAL_OK;
+}
+
+static void grid_free(GridImpl &g) {
+    if (g.dev >= 0) cudaSetDevice(g.dev);
+    for (auto &e : g.ev)
+        if (e) cudaEventDestroy(e);
+    for (void *p : g.allocs) cudaFree(p);
+    g.allocs.clear();
+    if (g.stream) cudaStreamDestroy(g.stream);
+    g.stream = nullptr;
+}
+
+static int require_device(int dev) {
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess || count == 0) return set_error(SAL_ENODEV, "no CUDA device is available");
+    if (dev < 0 || dev >= count) return set_error(SAL_EINVAL, "device ordinal out of range");
+    CK(cudaSetDevice(dev));
+    return SAL_OK;
+}
+
+extern "C" int sal_grid_create(const sal_tree *t_, const sal_grid_desc *d, sal_grid **out) {
+    if (!t_ || !d || !out) return set_error(SAL_EINVAL, "null argument");
+    *out = nullptr;
+    const Tree &t = *static_cast<const Tree *>(t_);
+    if (d->point_count != t.n) return set_error(SAL_EINVAL, "point_count differs from the tree's");
+    if (!d->xs || !d->ys || !d->zs || !d->areas) return set_error(SAL_EINVAL, "null point arrays");
+    if (d->mode < SAL_MODE_DTT || d->mode > SAL_MODE_STT_CORRECT) return set_error(SAL_EINVAL, "unknown mode");
+    if (d->mode == SAL_MODE_DTT && d->list_count > 0 && !d->list) return set_error(SAL_EINVAL, "null list");
+    if (d->mode != SAL_MODE_DTT && ((d->pc_count > 0 && !d->pc_list) || (d->pp_count > 0 && !d->pp_list)))
+        return set_error(SAL_EINVAL, "null STT list");
+    int rc = require_device(d->device);
+    if (rc) return rc;
+    auto t0 = std::chrono::steady_clock::now();
+    sal_grid *G = new sal_grid();
+    GridImpl &g = G->g;
+    g.dev = d->device;
+    std::string err;
+    if (!plan_build(t, d->interp_degree, d->mode, d->list, d->list_count, d->pc_list, d->pc_count, d->pp_list,
+                    d->pp_count, &g.plan, &err)) {
+        delete G;
+        return set_error(SAL_EINVAL, err);
+    }
+    Plan &pl = g.plan;
+    const int n = pl.n, P = pl.P, nd = pl.d + 1;
+    g.nsrc = (int)pl.src_slot_panel.size();
+    g.ntgt = (int)pl.tgt_slot_panel.size();
+    g.rec_stride = 4 * P + 2 * nd;
+    g.rec_stride = (g.rec_stride + 3) & ~3;  // records start on 32-byte boundaries
+    g.nup = (int)pl.up_units.size();
+    g.nproxy_units = (int)pl.proxy_groups.size();
+    if (cudaStreamCreateWithFlags(&g.stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete G;
+        return set_error(SAL_ECUDA, "cudaStreamCreate failed");
+    }
+#define TRY(x)                 \
+    do {                       \
+        int rc_ = (x);         \
+        if (rc_) {             \
+            grid_free(g);      \
+            delete G;          \
+            return rc_;        \
+        }                      \
+    } while (0)
+    {
+        std::vector<double4> xyz(n);
+        std::vector<double> area(n);
+        std::vector<double2> xe(n);
+        for (int p = 0; p < n; ++p) {
+            int i = pl.perm[p];
+            xyz[p] = make_double4(d->xs[i], d->ys[i], d->zs[i], 0.0);
+            area[p] = d->areas[i];
+            xe[p] = make_double2(pl.pxi[p], pl.peta[p]);
+        }
+        TRY(dupload(g, &g.xyz, xyz.data(), (size_t)n));
+        TRY(dupload(g, &g.area, area.data(), (size_t)n));
+        TRY(dupload(g, &g.xieta, xe.data(), (size_t)n));
+        TRY(dupload(g, &g.perm, pl.perm.data(), (size_t)n));
+        std::vector<double4> pool((size_t)n + (size_t)g.nsrc * P);
+        for (int p = 0; p < n; ++p) pool[p] = xyz[p];
+        for (size_t q = 0; q < (size_t)g.nsrc * P; ++q)
+            pool[n + q] = make_double4(pl.src_proxy_xyz[3 * q], pl.src_proxy_xyz[3 * q + 1], pl.src_proxy_xyz[3 * q + 2], 0.0);
+        TRY(dupload(g, &g.pool, pool.data(), pool.size()));
+        std::vector<double4> tp((size_t)g.ntgt * P);
+        for (size_t q = 0; q < tp.size(); ++q)
+            tp[q] = make_double4(pl.tgt_proxy_xyz[3 * q], pl.tgt_proxy_xyz[3 * q + 1], pl.tgt_proxy_xyz[3 * q + 2], 0.0);
+        TRY(dupload(g, &g.tgt_proxy, tp.data(), tp.size()));
+        std::vector<double> rec((size_t)g.ntgt * g.rec_stride, 0.0);
+        for (int s = 0; s < g.ntgt; ++s)
+            for (int i = 0; i < 2 * nd; ++i) rec[(size_t)s * g.rec_stride + 4 * P + i] = pl.tgt_nodes[(size_t)s * 2 * nd + i];
+        TRY(dupload(g, &g.records, rec.data(), rec.size()));
+    }
+    TRY(dupload(g, &g.leaf_groups, pl.leaf_groups.data(), pl.leaf_groups.size()));
+    TRY(dupload(g, &g.leaf_items, pl.leaf_items.data(), pl.leaf_items.size()));
+    TRY(dupload(g, &g.masks, pl.masks.data(), pl.masks.size()));
+    TRY(dupload(g, &g.proxy_groups, pl.proxy_groups.data(), pl.proxy_groups.size()));
+    TRY(dupload(g, &g.proxy_items, pl.proxy_items.data(), pl.proxy_items.size()));
+    TRY(dupload(g, &g.proxy_unit_beg, pl.proxy_unit_beg.data(), pl.proxy_unit_beg.size()));
+    TRY(dalloc(g, &g.proxy_partial, (size_t)g.nproxy_units * P));
+    TRY(dupload(g, &g.up_units, pl.up_units.data(), pl.up_units.size()));
+    TRY(dupload(g, &g.up_unit_beg, pl.up_unit_beg.data(), pl.up_unit_beg.size()));
+    TRY(dupload(g, &g.src_nodes, pl.src_nodes.data(), pl.src_nodes.size()));
+    TRY(dalloc(g, &g.up_partial, (size_t)g.nup * P));
+    TRY(dalloc(g, &g.err, 1));
+    CK(cudaMemset(g.err, 0, sizeof(int)));
+    CK(cudaDeviceSynchronize());
+    // host copies no longer needed on the device side
+    pl.px.clear(); pl.py.clear(); pl.pz.clear(); pl.parea.clear();
+    g.setup_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    *out = G;
+    return SAL_OK;
+#undef TRY
+}
+
+extern "C" int sal_grid_destroy(sal_grid *G) {
+    if (!G) return SAL_OK;
+    grid_free(G->g);
+    delete G;
+    return SAL_OK;
+}
+
+extern "C" int sal_grid_stats_get(const sal_grid *G, sal_grid_stats *s) {
+    if (!G || !s) return set_error(SAL_EINVAL, "null argument");
+    const GridImpl &g = G->g;
+    const Plan &pl = g.plan;
+    std::memset(s, 0, sizeof(*s));
+    s->point_count = pl.n;
+    s->npanels = pl.npanels;
+    s->nleaves = pl.nleaves;
+    s->degree = pl.d;
+    s->mode = pl.mode;
+    s->list_count = (int64_t)pl.leaf_items.size();
+    s->pairs_pp = pl.pairs[0];
+    s->pairs_pc = pl.pairs[1];
+    s->pairs_cp = pl.pairs[2];
+    s->pairs_cc = pl.pairs[3];
+    s->macs_up = pl.macs_up;
+    s->macs_down = pl.macs_down;
+    s->device_bytes = g.bytes;
+    s->setup_seconds = g.setup_seconds;
+    return SAL_OK;
+}
+
+// One FP64 solve of one field: ssh (caller order, device) -> outputs (caller order, device).
+static void solve_fp64(GridImpl &g, const double *ssh, double *ox, double *oy, int form, int kinds, bool do_up,
+                       cudaStream_t st) {
+    const Plan &pl = g.plan;
+    const int n = pl.n, P = pl.P;
+    if (g.timing) cudaEventRecord(g.ev[0], st);
+    dev::launch_prep(g.xyz, g.area, ssh, g.perm, n, g.pool, st);
+    if (do_up && g.nup > 0) {
+        dev::UpArgs u{g.pool, g.xieta, g.up_units, g.src_nodes, pl.d, P, g.up_partial};
+        dev::launch_upward(u, g.nup, st);
+        dev::launch_upward_finalize(g.up_unit_beg, g.up_partial, g.nsrc, pl.d, pl.mode == SAL_MODE_STT_REF_COMPAT ? 1 : 0,
+                                    g.pool + n, st);
+    }
+    if (g.timing) cudaEventRecord(g.ev[1], st);
+    if (g.nproxy_units > 0) {
+        dev::EvalArgs a{};
+        a.pool = g.pool;
+        a.groups = g.proxy_groups;
+        a.items = g.proxy_items;
+        a.masks = g.masks;
+        a.tgt = g.tgt_proxy;
+        a.xieta = g.xieta;
+        a.records = g.records;
+        a.rec_stride = g.rec_stride;
+        a.d = pl.d;
+        a.P = P;
+        a.kinds = 3;
+        a.perm = g.perm;
+        a.partial = g.proxy_partial;
+        a.err = g.err;
+        dev::launch_eval(1, form, a, g.nproxy_units, st);
+        dev::launch_proxy_finalize(g.proxy_unit_beg, g.proxy_partial, g.ntgt, P, g.rec_stride, g.records, st);
+    }
+    if (g.timing) cudaEventRecord(g.ev[2], st);
+    dev::EvalArgs a{};
+    a.pool = g.pool;
+    a.groups = g.leaf_groups;
+    a.items = g.leaf_items;
+    a.masks = g.masks;
+    a.tgt = g.pool;
+    a.xieta = g.xieta;
+    a.records = g.records;
+    a.rec_stride = g.rec_stride;
+    a.d = pl.d;
+    a.P = P;
+    a.kinds = kinds;
+    a.perm = g.perm;
+    a.out_x = ox;
+    a.out_y = oy;
+    a.err = g.err;
+    dev::launch_eval(0, form, a, (int)pl.leaf_groups.size(), st);
+    if (g.timing) {
+        cudaEventRecord(g.ev[3], st);
+        cudaEventSynchronize(g.ev[3]);
+        float t01 = 0, t12 = 0, t23 = 0;
+        cudaEventElapsedTime(&t01, g.ev[0], g.ev[1]);
+        cudaEventElapsedTime(&t12, g.ev[1], g.ev[2]);
+        cudaEventElapsedTime(&t23, g.ev[2], g.ev[3]);
+        g.phase_ms[0] += t01;
+        g.phase_ms[1] += t12;
+        g.phase_ms[2] += t23;
+        g.phase_ms[3] += t01 + t12 + t23;
+        g.phase_solves += 1;
+    }
+}
+
+extern "C" int sal_solve(sal_grid *G, const double *ssh, int32_t nf, int64_t ld_ssh, double *ox, double *oy,
+                         int64_t ld_out, int32_t form, void *stream) {
+    if (!G || !ssh || !ox || !oy) return set_error(SAL_EINVAL, "null argument");
+    GridImpl &g = G->g;
+    if (nf < 1) return set_error(SAL_EINVAL, "nfields must be >= 1");
+    if (nf > 1 && (ld_ssh < g.plan.n || ld_out < g.plan.n)) return set_error(SAL_EINVAL, "leading dimension < point_count");
+    if (form != SAL_FORM_REF && form != SAL_FORM_ACCURATE) return set_error(SAL_EINVAL, "unsupported form");
+    CK(cudaSetDevice(g.dev));
+    cudaStream_t st = stream ? (cudaStream_t)stream : g.stream;
+    for (int f = 0; f < nf; ++f)
+        solve_fp64(g, ssh + (size_t)f * ld_ssh, ox + (size_t)f * ld_out, oy + (size_t)f * ld_out,
+                   g.plan.mode == SAL_MODE_DTT ? form : SAL_FORM_REF, 7, true, st);
+    CK(cudaGetLastError());
+    return SAL_OK;
+}
+
+// Synchronises the grid's work on `stream` and reports a kernel time-out.
+static int finish(GridImpl &g, cudaStream_t st) {
+    CK(cudaStreamSynchronize(st));
+    int flag = 0;
+    CK(cudaMemcpy(&flag, g.err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (flag) {
+        cudaMemset(g.err, 0, sizeof(int));
+        return set_error(SAL_ETIMEOUT, "a staging wait timed out on the device");
+    }
+    return SAL_OK;
+}
+
+extern "C" int sal_grid_timing(sal_grid *G, int32_t enable, double *phase_ms, int64_t *solves) {
+    if (!G) return set_error(SAL_EINVAL, "null argument");
+    GridImpl &g = G->g;
+    CK(cudaSetDevice(g.dev));
+    if (phase_ms)
+        for (int i = 0; i < 4; ++i) phase_ms[i] = g.phase_ms[i];
+    if (solves) *solves = g.phase_solves;
+    if (enable >= 0) {
+        if (enable && !g.ev[0])
+            for (auto &e : g.ev) CK(cudaEventCreate(&e));
+        g.timing = enable != 0;
+        for (double &v : g.phase_ms) v = 0;
+        g.phase_solves = 0;
+    }
+    return SAL_OK;
+}
+
+extern "C" int sal_grid_sync(sal_grid *G, void *stream) {
+    if (!G) return set_error(SAL_EINVAL, "null argument");
+    CK(cudaSetDevice(G->g.dev));
+    return finish(G->g, stream ? (cudaStream_t)stream : G->g.stream);
+}
+
+static int ensure_host_staging(GridImpl &g) {
+    if (g.h_ssh) return SAL_OK;
+    const size_t n = (size_t)g.plan.n;
+    int rc = dalloc(g, &g.h_ssh, n);
+    if (!rc) rc = dalloc(g, &g.h_ox, n);
+    if (!rc) rc = dalloc(g, &g.h_oy, n);
+    if (!rc) rc = dalloc(g, &g.h_w, (size_t)g.plan.P * std::max(1, g.nsrc));
+    return rc;
+}
+
+// Adds device results into the caller's intent(inout) host arrays.
+static int add_back(GridImpl &g, double *hx, double *hy) {
+    const size_t n = (size_t)g.plan.n;
+    std::vector<double> tx(n), ty(n);
+    CK(cudaMemcpyAsync(tx.data(), g.h_ox, n * 8, cudaMemcpyDeviceToHost, g.stream));
+    CK(cudaMemcpyAsync(ty.data(), g.h_oy, n * 8, cudaMemcpyDeviceToHost, g.stream));
+    int rc = finish(g, g.stream);
+    if (rc) return rc;
+    for (size_t i = 0; i < n; ++i) {
+        hx[i] += tx[i];
+        hy[i] += ty[i];
+    }
+    return SAL_OK;
+}
+
+extern "C" int sal_fast_sum_host(sal_grid *G, const double *ssh, double *lon, double *lat, int32_t form) {
+    if (!G || !ssh || !lon || !lat) return set_error(SAL_EINVAL, "null argument");
+    GridImpl &g = G->g;
+    if (g.plan.mode != SAL_MODE_DTT) return set_error(SAL_EINVAL, "fast_sum needs a SAL_MODE_DTT grid");
+    if (form != SAL_FORM_REF && form != SAL_FORM_ACCURATE) return set_error(SAL_EINVAL, "unsupported form");
+    std::lock_guard<std::mutex> lk(g.mu);
+    CK(cudaSetDevice(g.dev));
+    int rc = ensure_host_staging(g);
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(g.h_ssh, ssh, (size_t)g.plan.n * 8, cudaMemcpyHostToDevice, g.stream));
+    solve_fp64(g, g.h_ssh, g.h_ox, g.h_oy, form, 7, true, g.stream);
+    CK(cudaGetLastError());
+    return add_back(g, lon, lat);
+}
+
+extern "C" int sal_proxy_source_compute_host(sal_grid *G, const double *sshs, double *weights) {
+    if (!G || !sshs || !weights) return set_error(SAL_EINVAL, "null argument");
+    GridImpl &g = G->g;
+    if (g.plan.mode == SAL_MODE_DTT) return set_error(SAL_EINVAL, "proxy_source_compute needs an STT grid");
+    std::lock_guard<std::mutex> lk(g.mu);
+    CK(cudaSetDevice(g.dev));
+    int rc = ensure_host_staging(g);
+    if (rc) return rc;
+    const Plan &pl = g.plan;
+    const int n = pl.n, P = pl.P;
+    CK(cudaMemcpyAsync(g.h_ssh, sshs, (size_t)n * 8, cudaMemcpyHostToDevice, g.stream));
+    dev::launch_prep(g.xyz, g.area, g.h_ssh, g.perm, n, g.pool, g.stream);
+    dev::UpArgs u{g.pool, g.xieta, g.up_units, g.src_nodes, pl.d, P, g.up_partial};
+    dev::launch_upward(u, g.nup, g.stream);
+    dev::launch_upward_finalize(g.up_unit_beg, g.up_partial, g.nsrc, pl.d, pl.mode == SAL_MODE_STT_REF_COMPAT ? 1 : 0,
+                                g.pool + n, g.stream);
+    const size_t cnt = (size_t)P * g.nsrc;
+    dev::launch_extract_w(g.pool + n, (int)cnt, g.h_w, g.stream);
+    std::vector<double> w(cnt);
+    CK(cudaMemcpyAsync(w.data(), g.h_w, cnt * 8, cudaMemcpyDeviceToHost, g.stream));
+    rc = finish(g, g.stream);
+    if (rc) return rc;
+    for (size_t i = 0; i < cnt; ++i) weights[i] += w[i];
+    return SAL_OK;
+}
+
+extern "C" int sal_pc_compute_host(sal_grid *G, const double *weights, double *sx, double *sy) {
+    if (!G || !weights || !sx || !sy) return set_error(SAL_EINVAL, "null argument");
+    GridImpl &g = G->g;
+    if (g.plan.mode == SAL_MODE_DTT) return set_error(SAL_EINVAL, "pc_compute needs an STT grid");
+    std::lock_guard<std::mutex> lk(g.mu);
+    CK(cudaSetDevice(g.dev));
+    int rc = ensure_host_staging(g);
+    if (rc) return rc;
+    const size_t cnt = (size_t)g.plan.P * g.nsrc;
+    CK(cudaMemcpyAsync(g.h_w, weights, cnt * 8, cudaMemcpyHostToDevice, g.stream));
+    dev::launch_insert_w(g.h_w, (int)cnt, g.pool + g.plan.n, g.stream);
+    // PC items only: point weights are not read, so no prep is needed
+    dev::EvalArgs a{};
+    a.pool = g.pool; a.groups = g.leaf_groups; a.items = g.leaf_items; a.masks = g.masks; a.tgt = g.pool;
+    a.xieta = g.xieta; a.records = g.records; a.rec_stride = g.rec_stride; a.d = g.plan.d; a.P = g.plan.P;
+    a.kinds = 2; a.perm = g.perm; a.out_x = g.h_ox; a.out_y = g.h_oy; a.err = g.err;
+    dev::launch_eval(0, SAL_FORM_REF, a, (int)g.plan.leaf_groups.size(), g.stream);
+    CK(cudaGetLastError());
+    return add_back(g, sx, sy);
+}
+
+extern "C" int sal_pp_compute_host(sal_grid *G, const double *sshs, double *sx, double *sy) {
+    if (!G || !sshs || !sx || !sy) return set_error(SAL_EINVAL, "null argument");
+    GridImpl &g = G->g;
+    if (g.plan.mode == SAL_MODE_DTT) return set_error(SAL_EINVAL, "pp_compute needs an STT grid");
+    std::lock_guard<std::mutex> lk(g.mu);
+    CK(cudaSetDevice(g.dev));
+    int rc = ensure_host_staging(g);
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(g.h_ssh, sshs, (size_t)g.plan.n * 8, cudaMemcpyHostToDevice, g.stream));
+    dev::launch_prep(g.xyz, g.area, g.h_ssh, g.perm, g.plan.n, g.pool, g.stream);
+    dev::EvalArgs a{};
+    a.pool = g.pool; a.groups = g.leaf_groups; a.items = g.leaf_items; a.masks = g.masks; a.tgt = g.pool;
+    a.xieta = g.xieta; a.records = g.records; a.rec_stride = g.rec_stride; a.d = g.plan.d; a.P = g.plan.P;
+    a.kinds = 1; a.perm = g.perm; a.out_x = g.h_ox; a.out_y = g.h_oy; a.err = g.err;
+    dev::launch_eval(0, SAL_FORM_REF, a, (int)g.plan.leaf_groups.size(), g.stream);
+    CK(cudaGetLastError());
+    return add_back(g, sx, sy);
+}
+
+// Scratch of the direct sum: per-device lazily grown buffer.
+static std::mutex g_direct_mu;
+static double *g_direct_scratch[64] = {nullptr};
+static size_t g_direct_cap[64] = {0};
+
+extern "C" int sal_direct_sum(const double *xs, const double *ys, const double *zs, const double *w, int32_t n,
+                              const int32_t *targets, int32_t nt, double *ox, double *oy, void *stream) {
+    if (!xs || !ys || !zs || !w || !targets || !ox || !oy) return set_error(SAL_EINVAL, "null argument");
+    if (n < 0 || nt < 0) return set_error(SAL_EINVAL, "negative size");
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    if (dev >= 64) return set_error(SAL_EINVAL, "device ordinal >= 64");
+    const int nch = dev::direct_chunks(n);
+    const size_t need = (size_t)nch * (size_t)nt * 2;
+    std::lock_guard<std::mutex> lk(g_direct_mu);
+    if (g_direct_cap[dev] < need) {
+        if (g_direct_scratch[dev]) cudaFree(g_direct_scratch[dev]);
+        g_direct_scratch[dev] = nullptr;
+        g_direct_cap[dev] = 0;
+        if (cudaMalloc((void **)&g_direct_scratch[dev], need * 8) != cudaSuccess)
+            return set_error(SAL_ENOMEM, "direct-sum scratch allocation failed");
+        g_direct_cap[dev] = need;
+    }
+    dev::launch_direct(xs, ys, zs, w, n, targets, nt, ox, oy, g_direct_scratch[dev], nch, (cudaStream_t)stream);
+    CK(cudaGetLastError());
+    return SAL_OK;
+}

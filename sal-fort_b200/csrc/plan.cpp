@@ -1,0 +1,295 @@
+// Flattening of a tree and its interaction lists into the device work plan.
+//
+// The device never walks the tree.  Every solve is four data-parallel passes
+// over flat arrays built here once per grid:
+//   upward   : per (source slot, chunk) unit, proxy weights W from the slot
+//              panel's points (fast_sum_module.f90:99-111,
+//              mom6_fast_sum_module.f90:33-74);
+//   proxy    : per target slot, proxy potentials at the target panel's
+//              Chebyshev nodes from CP sources (points) and CC sources
+//              (proxies) (fast_sum_module.f90:172-183, :254-271);
+//   leaf     : per leaf, PP sources (points) and PC sources (proxies) of the
+//              leaf and all its ancestors, plus one DOWN item per ancestor
+//              target slot that interpolates the proxy potentials
+//              (fast_sum_module.f90:58-72, :113-129, :185-199).
+// All sources live in one pool of (x, y, z, w) records: the n points in
+// leaf-contiguous order, then (d+1)^2 proxies per source slot, so every item
+// is a contiguous pool range the kernels stage with one bulk copy.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "sal_internal.hpp"
+
+namespace sal {
+
+static constexpr int kUpChunk = 4096;          // points per upward unit
+static constexpr double kProxyUnitPairs = 81.0 * 8192.0;  // pair budget of one proxy work unit
+
+static void panel_proxies(const Panel &q, int d, double *xyz, double *nodes, double *box) {
+    int n = d + 1;
+    double cx[kMaxDegree + 1], ce[kMaxDegree + 1];
+    cheb_nodes(q.min_xi, q.max_xi, d, cx);
+    cheb_nodes(q.min_eta, q.max_eta, d, ce);
+    // proxy p = i + j*n sits at (xi_i, eta_j): the loop order of
+    // fast_sum_module.f90:119-127 and mom6_fast_sum_module.f90:96-105
+    for (int j = 0; j < n; ++j)
+        for (int i = 0; i < n; ++i) {
+            double *o = xyz + 3 * (i + j * n);
+            xyz_from_xieta(cx[i], ce[j], q.face, &o[0], &o[1], &o[2]);
+        }
+    if (nodes) {
+        for (int i = 0; i < n; ++i) { nodes[i] = cx[i]; nodes[n + i] = ce[i]; }
+    }
+    if (box) { box[0] = q.min_xi; box[1] = q.max_xi; box[2] = q.min_eta; box[3] = q.max_eta; }
+}
+
+static void push_range(std::vector<Item> &v, int64_t off, int64_t cnt, int kind, int32_t mask) {
+    for (int64_t b = 0; b < cnt; b += kMaxStage) {
+        int64_t c = std::min<int64_t>(kMaxStage, cnt - b);
+        v.push_back(Item{(int32_t)(off + b), (int32_t)c, mask, kind});
+    }
+}
+
+bool plan_build(const Tree &t, int d, int mode, const int32_t *list, int64_t nlist, const int32_t *pc, int64_t npc,
+                const int32_t *pp, int64_t npp, Plan *pl, std::string *err) {
+    if (d < 1 || d > kMaxDegree) { *err = "interp_degree must be in 1.." + std::to_string(kMaxDegree); return false; }
+    const int n = t.n, np = (int)t.p.size(), nd = d + 1, P = nd * nd;
+    pl->n = n; pl->d = d; pl->P = P; pl->mode = mode; pl->npanels = np;
+    pl->perm = t.order;
+    // ---------------------------------------------------------------- leaves
+    std::vector<int32_t> leaves;                 // panel indices of leaves with points, by range start
+    for (int k = 0; k < np; ++k)
+        if (t.p[k].is_leaf && t.p[k].count() > 0) leaves.push_back(k);
+    std::sort(leaves.begin(), leaves.end(), [&](int a, int b) { return t.p[a].begin < t.p[b].begin; });
+    pl->nleaves = (int)leaves.size();
+    std::vector<int64_t> leaf_begin(leaves.size());
+    for (size_t i = 0; i < leaves.size(); ++i) leaf_begin[i] = t.p[leaves[i]].begin;
+    for (auto k : leaves)
+        if (t.p[k].count() > 256) { *err = "leaves with more than 256 points are not supported (cluster_thresh <= 257)"; return false; }
+    // leaves under panel k: contiguous in range order
+    auto leaf_range = [&](int k, int32_t *lb, int32_t *le) {
+        const Panel &q = t.p[k];
+        *lb = (int32_t)(std::lower_bound(leaf_begin.begin(), leaf_begin.end(), q.begin) - leaf_begin.begin());
+        *le = (int32_t)(std::lower_bound(leaf_begin.begin(), leaf_begin.end(), q.end) - leaf_begin.begin());
+    };
+    std::vector<int32_t> leaf_of_pos(n, -1);
+    for (size_t i = 0; i < leaves.size(); ++i)
+        for (int64_t p = t.p[leaves[i]].begin; p < t.p[leaves[i]].end; ++p) leaf_of_pos[p] = (int32_t)i;
+    // ---------------------------------------------------------------- slots
+    std::vector<int32_t> src_slot(np, -1), tgt_slot(np, -1);
+    const bool dtt = (mode == 0);
+    if (dtt) {
+        for (int64_t i = 0; i < nlist; ++i) {
+            int32_t it = list[3 * i], is = list[3 * i + 1], ty = list[3 * i + 2];
+            if (it < 1 || it > np || is < 1 || is > np || ty < 0 || ty > 3) {
+                *err = "interaction " + std::to_string(i + 1) + " is out of range";
+                return false;
+            }
+            if (ty == 1 || ty == 3) src_slot[is - 1] = 0;
+            if (ty == 2 || ty == 3) tgt_slot[it - 1] = 0;
+        }
+    } else {
+        for (int k = 0; k < np; ++k) src_slot[k] = 0;  // slot == panel index: the reference's flat weight layout
+    }
+    for (int k = 0; k < np; ++k)
+        if (src_slot[k] == 0) { src_slot[k] = (int32_t)pl->src_slot_panel.size(); pl->src_slot_panel.push_back(k); }
+    for (int k = 0; k < np; ++k)
+        if (tgt_slot[k] == 0) { tgt_slot[k] = (int32_t)pl->tgt_slot_panel.size(); pl->tgt_slot_panel.push_back(k); }
+    const int32_t nsrc = (int32_t)pl->src_slot_panel.size(), ntgt = (int32_t)pl->tgt_slot_panel.size();
+    if ((int64_t)n + (int64_t)nsrc * P > INT32_MAX / 2) { *err = "grid too large for 32-bit pool offsets"; return false; }
+    pl->src_proxy_xyz.resize((size_t)nsrc * P * 3);
+    pl->src_nodes.resize((size_t)nsrc * 2 * nd);
+    pl->src_box.resize((size_t)nsrc * 4);
+    for (int32_t s = 0; s < nsrc; ++s)
+        panel_proxies(t.p[pl->src_slot_panel[s]], d, &pl->src_proxy_xyz[(size_t)s * P * 3], &pl->src_nodes[(size_t)s * 2 * nd],
+                      &pl->src_box[(size_t)s * 4]);
+    pl->tgt_proxy_xyz.resize((size_t)ntgt * P * 3);
+    pl->tgt_nodes.resize((size_t)ntgt * 2 * nd);
+    pl->tgt_box.resize((size_t)ntgt * 4);
+    for (int32_t s = 0; s < ntgt; ++s)
+        panel_proxies(t.p[pl->tgt_slot_panel[s]], d, &pl->tgt_proxy_xyz[(size_t)s * P * 3], &pl->tgt_nodes[(size_t)s * 2 * nd],
+                      &pl->tgt_box[(size_t)s * 4]);
+    // ---------------------------------------------------------------- upward units
+    pl->up_unit_beg.assign(nsrc + 1, 0);
+    for (int32_t s = 0; s < nsrc; ++s) {
+        const Panel &q = t.p[pl->src_slot_panel[s]];
+        pl->up_unit_beg[s] = (int32_t)pl->up_units.size();
+        for (int64_t b = q.begin; b < q.end; b += kUpChunk)
+            pl->up_units.push_back(UpUnit{s, (int32_t)b, (int32_t)std::min<int64_t>(q.end, b + kUpChunk), pl->src_slot_panel[s]});
+        pl->macs_up += (double)q.count() * P;
+    }
+    pl->up_unit_beg[nsrc] = (int32_t)pl->up_units.size();
+    // ---------------------------------------------------------------- per-leaf and per-target-slot items
+    const int64_t pool_proxy0 = n;
+    auto proxy_off = [&](int k) { return pool_proxy0 + (int64_t)src_slot[k] * P; };
+    std::vector<std::vector<Item>> litems(leaves.size()), titems(ntgt);
+    std::vector<double> lcost(leaves.size(), 0.0), tcost(ntgt, 0.0);
+    pl->masks.clear();
+    if (dtt) {
+        for (int64_t i = 0; i < nlist; ++i) {
+            int k_t = list[3 * i] - 1, k_s = list[3 * i + 1] - 1, ty = list[3 * i + 2];
+            const Panel &T = t.p[k_t], &S = t.p[k_s];
+            if (T.count() == 0 || S.count() == 0) continue;
+            if (ty == 0 || ty == 1) {
+                int32_t lb, le;
+                leaf_range(k_t, &lb, &le);
+                for (int32_t l = lb; l < le; ++l) {
+                    if (ty == 0) push_range(litems[l], S.begin, S.count(), 0, -1);
+                    else push_range(litems[l], proxy_off(k_s), P, 1, -1);
+                    lcost[l] += (double)(ty == 0 ? S.count() : P) * t.p[leaves[l]].count();
+                }
+                pl->pairs[ty] += (double)T.count() * (ty == 0 ? S.count() : P);
+            } else {
+                int32_t ts = tgt_slot[k_t];
+                if (ty == 2) push_range(titems[ts], S.begin, S.count(), 0, -1);
+                else push_range(titems[ts], proxy_off(k_s), P, 1, -1);
+                tcost[ts] += (double)P * (ty == 2 ? S.count() : P);
+                pl->pairs[ty] += (double)P * (ty == 2 ? S.count() : P);
+            }
+        }
+        // DOWN items: every leaf under a target slot interpolates its potentials
+        for (int32_t s = 0; s < ntgt; ++s) {
+            int32_t lb, le;
+            leaf_range(pl->tgt_slot_panel[s], &lb, &le);
+            for (int32_t l = lb; l < le; ++l) {
+                litems[l].push_back(Item{s, 0, -1, 2});
+                lcost[l] += (double)P * t.p[leaves[l]].count() * 0.5;
+            }
+            pl->macs_down += (double)t.p[pl->tgt_slot_panel[s]].count() * P;
+        }
+    } else {
+        // STT: per-point pairs become per-leaf items with per-target bitmasks.
+        struct PairRec { int32_t key, local; };
+        for (int64_t i = 0; i < npc + npp; ++i) {
+            const int32_t *e = i < npc ? pc + 2 * i : pp + 2 * (i - npc);
+            if (e[0] < 1 || e[0] > n || e[1] < 1 || e[1] > np) { *err = "STT list entry out of range"; return false; }
+        }
+        std::vector<int32_t> pos_of(n);
+        for (int32_t p = 0; p < n; ++p) pos_of[t.order[p]] = p;
+        // bucket pairs by leaf: key = panel*2 + kind
+        std::vector<int64_t> off(leaves.size() + 1, 0);
+        auto leaf_of_point = [&](int32_t ip) { return leaf_of_pos[pos_of[ip]]; };
+        for (int64_t i = 0; i < npc; ++i) off[leaf_of_point(pc[2 * i] - 1) + 1]++;
+        for (int64_t i = 0; i < npp; ++i) off[leaf_of_point(pp[2 * i] - 1) + 1]++;
+        for (size_t l = 0; l < leaves.size(); ++l) off[l + 1] += off[l];
+        std::vector<PairRec> recs(off.back());
+        {
+            std::vector<int64_t> w(off.begin(), off.end() - 1);
+            auto put = [&](const int32_t *L, int64_t m, int kind) {
+                for (int64_t i = 0; i < m; ++i) {
+                    int32_t ip = L[2 * i] - 1, is = L[2 * i + 1] - 1;
+                    int32_t pos = pos_of[ip], l = leaf_of_pos[pos];
+                    recs[w[l]++] = PairRec{is * 2 + kind, (int32_t)(pos - t.p[leaves[l]].begin)};
+                }
+            };
+            put(pc, npc, 1);
+            put(pp, npp, 0);
+        }
+        std::vector<std::vector<uint32_t>> lmask(leaves.size());
+#pragma omp parallel for schedule(dynamic, 16)
+        for (int64_t l = 0; l < (int64_t)leaves.size(); ++l) {
+            const int64_t nt = t.p[leaves[l]].count();
+            const int words = (int)((nt + 31) / 32);
+            std::unordered_map<int32_t, int32_t> idx;
+            std::vector<int32_t> keys;
+            std::vector<uint32_t> &mk = lmask[l];
+            for (int64_t r = off[l]; r < off[l + 1]; ++r) {
+                auto it = idx.find(recs[r].key);
+                int32_t slot;
+                if (it == idx.end()) {
+                    slot = (int32_t)keys.size();
+                    idx.emplace(recs[r].key, slot);
+                    keys.push_back(recs[r].key);
+                    mk.resize(mk.size() + words, 0u);
+                } else {
+                    slot = it->second;
+                }
+                mk[(size_t)slot * words + recs[r].local / 32] |= 1u << (recs[r].local % 32);
+            }
+            // emit items in (kind, panel) order for locality; mask offsets are
+            // leaf-local here and rebased below
+            std::vector<int32_t> ordk(keys.size());
+            std::iota(ordk.begin(), ordk.end(), 0);
+            std::sort(ordk.begin(), ordk.end(), [&](int a, int b) { return keys[a] < keys[b]; });
+            double c = 0;
+            for (int32_t a : ordk) {
+                int32_t k_s = keys[a] / 2, kind = keys[a] % 2;
+                if (kind == 0) push_range(litems[l], t.p[k_s].begin, t.p[k_s].count(), 0, a * words);
+                else push_range(litems[l], proxy_off(k_s), P, 1, a * words);
+                c += (double)(kind == 0 ? t.p[k_s].count() : P) * nt;
+            }
+            lcost[l] = c;
+        }
+        for (size_t l = 0; l < leaves.size(); ++l) {
+            int32_t base = (int32_t)pl->masks.size();
+            for (auto &it : litems[l]) it.mask += base;
+            pl->masks.insert(pl->masks.end(), lmask[l].begin(), lmask[l].end());
+        }
+        for (int64_t i = 0; i < npc; ++i) pl->pairs[1] += P;
+        for (int64_t i = 0; i < npp; ++i) pl->pairs[0] += (double)t.p[pp[2 * i + 1] - 1].count();
+    }
+    // ---------------------------------------------------------------- groups, sorted by cost
+    {
+        std::vector<int32_t> ord(leaves.size());
+        std::iota(ord.begin(), ord.end(), 0);
+        std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) { return lcost[a] > lcost[b]; });
+        pl->leaf_groups.clear();
+        pl->leaf_items.clear();
+        pl->max_nt = 0;
+        for (int32_t l : ord) {
+            const Panel &L = t.p[leaves[l]];
+            Group g{};
+            g.tgt = (int32_t)L.begin; g.nt = (int32_t)L.count();
+            g.ib = (int32_t)pl->leaf_items.size();
+            pl->leaf_items.insert(pl->leaf_items.end(), litems[l].begin(), litems[l].end());
+            g.ie = (int32_t)pl->leaf_items.size();
+            g.out = l;
+            pl->max_nt = std::max(pl->max_nt, g.nt);
+            pl->leaf_groups.push_back(g);
+        }
+    }
+    {
+        // proxy groups: each target slot's items split into units of bounded work
+        pl->proxy_groups.clear();
+        pl->proxy_items.clear();
+        pl->proxy_unit_beg.assign(ntgt + 1, 0);
+        std::vector<Group> units;
+        std::vector<double> ucost;
+        for (int32_t s = 0; s < ntgt; ++s) {
+            pl->proxy_unit_beg[s] = (int32_t)units.size();
+            const auto &v = titems[s];
+            size_t i = 0;
+            while (i < v.size()) {
+                Group g{};
+                g.tgt = s; g.nt = P;
+                g.ib = (int32_t)pl->proxy_items.size();
+                double c = 0;
+                while (i < v.size() && (c == 0 || c + (double)v[i].cnt * P <= kProxyUnitPairs)) {
+                    pl->proxy_items.push_back(v[i]);
+                    c += (double)v[i].cnt * P;
+                    ++i;
+                }
+                g.ie = (int32_t)pl->proxy_items.size();
+                g.out = (int32_t)units.size();
+                units.push_back(g);
+                ucost.push_back(c);
+            }
+        }
+        pl->proxy_unit_beg[ntgt] = (int32_t)units.size();
+        std::vector<int32_t> ord(units.size());
+        std::iota(ord.begin(), ord.end(), 0);
+        std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) { return ucost[a] > ucost[b]; });
+        for (int32_t u : ord) pl->proxy_groups.push_back(units[u]);
+    }
+    // ---------------------------------------------------------------- point data in pool order
+    pl->pxi.resize(n); pl->peta.resize(n);
+    for (int32_t p = 0; p < n; ++p) { pl->pxi[p] = t.xi[t.order[p]]; pl->peta[p] = t.eta[t.order[p]]; }
+    return true;
+}
+
+}  // namespace sal

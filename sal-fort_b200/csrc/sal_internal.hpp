@@ -1,0 +1,109 @@
+// Internal host-side types of libsalgpu: the cubed-sphere tree, interaction
+// lists and the flattened device work plan.
+#pragma once
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace sal {
+
+// One panel of the cubed-sphere quadtree (tree_module.f90:5-28).  Panels live
+// in BFS order with children contiguous, so panel id k (1-based, as in the
+// reference) is Tree::p[k-1].  Instead of a points_inside array per panel,
+// every panel owns the contiguous range [begin, end) of Tree::order: the tree
+// builder partitions points stably, so a leaf's range lists its points in the
+// reference's points_inside order, and an internal panel's range holds the same
+// set as its points_inside.
+struct Panel {
+    int32_t level = 0, is_leaf = 1, id = 0, parent = -1;
+    int32_t child[4] = {-1, -1, -1, -1};
+    int32_t face = 0;
+    double min_xi = 0, mid_xi = 0, max_xi = 0, min_eta = 0, mid_eta = 0, max_eta = 0, radius = 0;
+    int64_t begin = 0, end = 0;
+    int64_t count() const { return end - begin; }
+};
+
+struct Tree {
+    int32_t n = 0;                 // points
+    std::vector<Panel> p;          // p[k] = panel id k+1
+    std::vector<int32_t> order;    // order[pos] = 0-based point index; panels own ranges of it
+    std::vector<double> xi, eta;   // per point (0-based), on the point's own face
+    std::vector<int8_t> face;      // per point
+    std::vector<double> cx, cy, cz; // per panel: xyz of (mid_xi, mid_eta), the MAC centre
+    int32_t max_level() const;
+    // Reference points_inside of panel id k (1-based ids, index-sorted).
+    std::vector<int32_t> points_inside(int32_t k) const;
+};
+
+// tree_module.f90 restated for the host.
+void face_xieta(double x, double y, double z, int face, double *xi, double *eta);
+void xyz_from_xieta(double xi, double eta, int face, double *x, double *y, double *z);
+int face_from_xyz(double x, double y, double z);
+void cheb_nodes(double min_x, double max_x, int degree, double *out);
+
+Tree *tree_build(const double *xs, const double *ys, const double *zs, int32_t n, int32_t thresh);
+Tree *tree_import(int32_t npanels, const int32_t *ints9, const double *dbl7, const int64_t *pt_off,
+                  const int32_t *pt_idx, int32_t n, const double *xs, const double *ys, const double *zs,
+                  std::string *err);
+void tree_set_points(Tree *t, const double *xs, const double *ys, const double *zs);
+std::vector<int32_t> dual_tree_traversal(const Tree &t, double theta, int32_t thresh);
+void single_tree_traversal(const Tree &t, double theta, int32_t thresh, const double *xs, const double *ys,
+                           const double *zs, int32_t own, std::vector<int32_t> *pc, std::vector<int32_t> *pp);
+int assign_points_to_panels(const Tree &t, const double *xs, const double *ys, const double *zs, int32_t own,
+                            int32_t *points_panels, int32_t nlev);
+
+// ---------------------------------------------------------------- work plan
+// Item of a target group's work list.  kind 0: sources are pool entries
+// [off, off+cnt) (points or proxies); kind 1: a DOWN item, interpolation from
+// target slot `off`.  mask: word offset of the per-target bitmask (STT), or -1.
+struct Item {
+    int32_t off, cnt, mask, kind;
+};
+
+struct Group {           // a set of targets with one work list
+    int32_t tgt;         // first target: pool position (leaf) or target-proxy slot (proxy group)
+    int32_t nt;          // number of targets
+    int32_t ib, ie;      // item range
+    int32_t out;         // partial-output slot (proxy groups) or unused
+    int32_t pad0, pad1, pad2;
+};
+
+struct UpUnit {          // upward-pass work unit
+    int32_t slot, beg, end, panel;
+};
+
+struct Plan {
+    int32_t n = 0, d = 0, P = 0, mode = 0, npanels = 0, nleaves = 0;
+    // point data in pool order (leaf-contiguous DFS)
+    std::vector<int32_t> perm;       // pos -> caller index
+    std::vector<double> px, py, pz, parea, pxi, peta;
+    // source proxy slots
+    std::vector<int32_t> src_slot_panel;          // slot -> panel index (0-based)
+    std::vector<double> src_proxy_xyz;            // slot*P*3
+    std::vector<UpUnit> up_units;
+    std::vector<int32_t> up_unit_beg;             // slot -> first unit (size nslots+1)
+    // target proxy slots (DTT CP/CC targets)
+    std::vector<int32_t> tgt_slot_panel;
+    std::vector<double> tgt_proxy_xyz;            // slot*P*3
+    std::vector<double> tgt_nodes;                // slot*2*(d+1): xi nodes then eta nodes
+    std::vector<double> tgt_box;                  // slot*4: min_xi,max_xi,min_eta,max_eta
+    std::vector<double> src_nodes, src_box;       // same for source slots (upward)
+    std::vector<Group> proxy_groups;              // work units of target slots, sorted by cost
+    std::vector<int32_t> proxy_unit_beg;          // tgt slot -> first unit (nslots+1); units in proxy_groups order by slot
+    std::vector<Item> proxy_items;
+    std::vector<Group> leaf_groups;               // one per leaf with targets, sorted by cost
+    std::vector<Item> leaf_items;
+    std::vector<uint32_t> masks;                  // STT per-target bitmasks
+    double pairs[4] = {0, 0, 0, 0};               // PP, PC, CP, CC evaluations per field
+    double macs_up = 0, macs_down = 0;
+    int32_t max_nt = 0;
+};
+
+// Builds the plan of a DTT list (triplets) or STT lists (pairs).
+bool plan_build(const Tree &t, int d, int mode, const int32_t *list, int64_t nlist, const int32_t *pc, int64_t npc,
+                const int32_t *pp, int64_t npp, Plan *plan, std::string *err);
+
+constexpr int kMaxStage = 256;   // sources staged per item (items are split to fit)
+constexpr int kMaxDegree = 15;   // (d+1)^2 <= 256 proxies
+
+}  // namespace sal
