@@ -150,7 +150,8 @@ int sal_grid_destroy(sal_grid *g);
 /* Batched solve on device buffers.  ssh: nfields columns of point_count
  * doubles, column f at ssh + f*ld_ssh, caller's point order.  Outputs likewise
  * (overwritten, not accumulated).  form is SAL_FORM_*; SAL_FORM_REF supports
- * nfields == 1 per column loop.  Asynchronous on stream. */
+ * nfields == 1 per column loop.  Asynchronous on stream (NULL: the CUDA
+ * default stream). */
 int sal_solve(sal_grid *g, const double *ssh, int32_t nfields, int64_t ld_ssh, double *out_x, double *out_y,
               int64_t ld_out, int32_t form, void *stream);
 

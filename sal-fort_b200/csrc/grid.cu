@@ -317,7 +317,7 @@ extern "C" int sal_solve(sal_grid *G, const double *ssh, int32_t nf, int64_t ld_
     if (nf > 1 && (ld_ssh < g.plan.n || ld_out < g.plan.n)) return set_error(SAL_EINVAL, "leading dimension < point_count");
     if (form != SAL_FORM_REF && form != SAL_FORM_ACCURATE) return set_error(SAL_EINVAL, "unsupported form");
     CK(cudaSetDevice(g.dev));
-    cudaStream_t st = stream ? (cudaStream_t)stream : g.stream;
+    cudaStream_t st = (cudaStream_t)stream;  // NULL: the CUDA default stream
     for (int f = 0; f < nf; ++f)
         solve_fp64(g, ssh + (size_t)f * ld_ssh, ox + (size_t)f * ld_out, oy + (size_t)f * ld_out,
                    g.plan.mode == SAL_MODE_DTT ? form : SAL_FORM_REF, 7, true, st);

@@ -142,8 +142,8 @@ __global__ void __launch_bounds__(kThreads) eval_kernel(EvalArgs a) {
         tgt_init(T, 0.0, 0.0, 0.5);
         T.live = false;
     }
-    double ax = 0.0, ay = 0.0, az = 0.0;  // PP/PC sums (proxy targets in FORM 1: Cartesian)
-    double ux = 0.0, uy = 0.0, uz = 0.0;  // DOWN sums in FORM 1 (Cartesian)
+    double ax = 0.0, ay = 0.0, az = 0.0;  // PP/PC sums, before the target factor (proxy targets in FORM 1: Cartesian)
+    double ux = 0.0, uy = 0.0, uz = 0.0;  // DOWN sums (FORM 0: east/north; FORM 1: Cartesian)
     if (tid == 0) {
         mbar_init(&bar[0], 1);
         mbar_init(&bar[1], 1);
@@ -188,8 +188,8 @@ __global__ void __launch_bounds__(kThreads) eval_kernel(EvalArgs a) {
                         const double bv = fx[jj] * fe[kk];
                         const double4 ph = S[jj + kk * n];
                         if (FORM == 0) {
-                            ax += bv * ph.x;
-                            ay += bv * ph.y;
+                            ux += bv * ph.x;
+                            uy += bv * ph.y;
                         } else {
                             ux += bv * ph.x;
                             uy += bv * ph.y;
@@ -213,15 +213,21 @@ __global__ void __launch_bounds__(kThreads) eval_kernel(EvalArgs a) {
                 } else {
                     for (int s = sp; s < it.cnt; s += nsplit) {
                         const double4 q = S[s];
-                        double gx, gy;
-                        gref(T, q.x, q.y, q.z, gx, gy);
-                        ax += gx * q.w;
-                        ay += gy * q.w;
+                        gref_fast(T, q.x, q.y, q.z, q.w, ax, ay);
                     }
                 }
             }
         }
         __syncthreads();
+    }
+    if (!(TGT == 1 && FORM == 1)) {
+        // the target factor 1/sqrt(1 - tz^2) of every pair sum (zero outside the pole guard)
+        ax *= T.live ? T.inv_mp2 : 0.0;
+        ay *= T.live ? T.inv_mp2 : 0.0;
+    }
+    if (TGT == 0 && FORM == 0) {
+        ax += ux;
+        ay += uy;
     }
     if (TGT == 0 && FORM == 1 && active && sp == 0 && T.live) {
         // project the interpolated Cartesian sum on the target's east/north frame
@@ -316,7 +322,7 @@ __global__ void __launch_bounds__(kDirectTile) direct_kernel(const double *__res
         if (T.live)
             for (int s = 0; s < m; ++s) {
                 double gx, gy;
-                gref(T, S[s].x, S[s].y, S[s].z, gx, gy);
+                gref_exact(T, S[s].x, S[s].y, S[s].z, gx, gy);
                 ax += gx * S[s].w;
                 ay += gy * S[s].w;
             }

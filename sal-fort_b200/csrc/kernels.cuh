@@ -77,10 +77,11 @@ __device__ __forceinline__ void tgt_init(Tgt &t, double x, double y, double z) {
 }
 
 // sal_grad_gfunc (fast_sum_module.f90:9-31) for a live target, operation for
-// operation and without contraction, so the singular self pair s == t rounds
-// exactly as the reference's does.  The division by sqrt(1-tz^2) is a multiply
-// by its hoisted reciprocal (one rounding of difference in a non-singular factor).
-__device__ __forceinline__ void gref(const Tgt &t, double sx, double sy, double sz, double &gx, double &gy) {
+// operation with IEEE division and square root and without contraction, so the
+// singular self pair s == t rounds exactly as the reference's does.  The
+// division by sqrt(1-tz^2) is a multiply by its hoisted reciprocal.  Used by
+// the direct sum, the accuracy judge.
+__device__ __forceinline__ void gref_exact(const Tgt &t, double sx, double sy, double sz, double &gx, double &gy) {
     double gxy = __dadd_rn(__dmul_rn(t.x, sx), __dmul_rn(t.y, sy));
     double g = __dadd_rn(gxy, __dmul_rn(t.z, sz));
     g = fmax(fmin(g, 1.0), -1.0);
@@ -96,17 +97,67 @@ __device__ __forceinline__ void gref(const Tgt &t, double sx, double sy, double 
     gx = __dmul_rn(__dmul_rn(nx, t.inv_mp2), val);
 }
 
+// Reciprocal and square root for the treecode's inner loops: an FP32
+// hardware approximation refined by Newton-Raphson iterations in FP64
+// (reciprocal: r <- r + r(1 - x r), twice; square root: one step of the
+// inverse-square-root iteration y <- y(3 - x y^2)/2, then one Heron step
+// s <- s + y(x - s^2)/2), accurate to about one ulp.  Valid for
+// 1e-37 < |x| < 1e37 (fast_rcp) and x == 0 or 1e-37 < x < 1e37 (fast_sqrt),
+// the ranges their callers produce.
+__device__ __forceinline__ double fast_rcp(double x) {
+    float xf = __double2float_rn(x), rf;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(rf) : "f"(xf));
+    double r = (double)rf;
+    double e = fma(-x, r, 1.0);
+    r = fma(r, e, r);
+    e = fma(-x, r, 1.0);
+    return fma(r, e, r);
+}
+__device__ __forceinline__ double fast_sqrt(double x) {
+    float xf = __double2float_rn(x), yf;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(yf) : "f"(xf));
+    double y = (double)yf;
+    double h = 0.5 * x;
+    y = y * fma(-h * y, y, 1.5);
+    double s = x * y;
+    s = fma(fma(-s, s, x), 0.5 * y, s);
+    return x > 0.0 ? s : 0.0;
+}
+
+// The reference kernel as the treecode evaluates it: g, mp = 2 - 2g, the two
+// denominators and the two numerators in the reference's exact operation
+// order (these carry the cancellations that make the self pair pure rounding
+// noise), p1 + p2 over one common denominator, and the target factor
+// 1/sqrt(1 - tz^2) left to the caller (applied once per target).  Adds the
+// un-normalised (nx, ny) * val * w into (ax, ay).
+__device__ __forceinline__ void gref_fast(const Tgt &t, double sx, double sy, double sz, double w, double &ax,
+                                          double &ay) {
+    double gxy = __dadd_rn(__dmul_rn(t.x, sx), __dmul_rn(t.y, sy));
+    double g = __dadd_rn(gxy, __dmul_rn(t.z, sz));
+    g = fmax(fmin(g, 1.0), -1.0);
+    double g2 = __dmul_rn(2.0, g);
+    double mp = __dsub_rn(2.0, g2);
+    double sqp = fast_sqrt(mp);
+    double d1 = __dadd_rn(__dmul_rn(sqp, mp), 1e-16);
+    double n2 = __dmul_rn(kC2, __dadd_rn(g2, sqp));
+    double d2 = __dadd_rn(__dmul_rn(2.0, __dsub_rn(__dmul_rn(g, g), 1.0)), 1e-16);
+    double val = fma(kC1, d2, n2 * d1) * fast_rcp(d1 * d2) * (kCons * w);
+    double ny = __dsub_rn(__dmul_rn(sz, t.omx32), __dmul_rn(t.z, gxy));
+    double nx = __dsub_rn(__dmul_rn(t.x, sy), __dmul_rn(t.y, sx));
+    ax = fma(nx, val, ax);
+    ay = fma(ny, val, ay);
+}
+
 // The scalar val of the kernel with its removable antipodal singularity
 // cancelled analytically (q = |t - s|):  2g + q = (2 - q)(1 + q) and
 // 2(g^2 - 1) = -q^2 (2 - q)(2 + q)/2, so p2 = -2 * 8.7 * (1 + q) / (q^2 (2 + q)).
 // mp = q^2 comes from coordinate differences, not from 2 - 2 t.s.
 __device__ __forceinline__ double vstable(double mp) {
-    double q = sqrt(mp);
+    double q = fast_sqrt(mp);
     double d1 = q * mp + 1e-16;
     double d2 = mp * (2.0 + q) + 1e-16;
-    // (kC1 / d1 + p2num / d2) with one division
     double num = kC1 * d2 - 2.0 * kC2 * (1.0 + q) * d1;
-    return kCons * num / (d1 * d2);
+    return kCons * num * fast_rcp(d1 * d2);
 }
 
 // bli_coeffs, bli_module.f90:6-26 (0-based index i0 of degree d).
