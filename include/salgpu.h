@@ -179,6 +179,26 @@ int sal_pp_compute_host(sal_grid *g, const double *sshs, double *sal_x, double *
 int sal_direct_sum(const double *xs, const double *ys, const double *zs, const double *w, int32_t n,
                    const int32_t *targets, int32_t nt, double *out_x, double *out_y, void *stream);
 
+/* Size of the fixed device scratch array behind sal_direct_sum_noalloc, in
+ * doubles (2 MiB): one call handles at most SAL_NOALLOC_SCRATCH_DOUBLES / 2
+ * targets. */
+#define SAL_NOALLOC_SCRATCH_DOUBLES (1 << 18)
+
+/* sal_direct_sum without any device allocation.  No counterpart in the
+ * reference: it exists for callers that cannot call cudaMalloc -- for example a
+ * thread running while another framework's caching allocator already holds the
+ * device's memory, or code that cannot accept the device-wide synchronisation
+ * cudaMalloc/cudaFree may cause.  Arguments and results are those of
+ * sal_direct_sum; the partial sums live in a fixed 2 MiB array in the
+ * library's device memory that every GPU loading the library keeps until the
+ * process exits.  nt above SAL_NOALLOC_SCRATCH_DOUBLES / 2 returns SAL_EINVAL.
+ * The first call on a device looks up that array's device address (make it
+ * before any stream capture).  All calls share the array: calls whose work
+ * overlaps on the GPU race and must be ordered by the caller (one stream, or
+ * events). */
+int sal_direct_sum_noalloc(const double *xs, const double *ys, const double *zs, const double *w, int32_t n,
+                           const int32_t *targets, int32_t nt, double *out_x, double *out_y, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -36,7 +36,7 @@ EXPORTS = (
     "sal_tree_destroy", "sal_dual_tree_traversal", "sal_single_tree_traversal", "sal_assign_points_to_panels",
     "sal_grid_create", "sal_grid_stats_get", "sal_grid_sync", "sal_grid_destroy", "sal_solve", "sal_fast_sum_host",
     "sal_proxy_source_compute_host", "sal_pc_compute_host", "sal_pp_compute_host", "sal_direct_sum",
-    "sal_grid_timing", "sal_fma_peak",
+    "sal_grid_timing", "sal_fma_peak", "sal_direct_sum_noalloc",
 )
 
 
@@ -109,6 +109,7 @@ def lib():
         L.sal_direct_sum.argtypes = [vp, vp, vp, vp, i32, vp, i32, vp, vp, vp]
         L.sal_grid_timing.argtypes = [vp, i32, C.POINTER(d), C.POINTER(i64)]
         L.sal_fma_peak.argtypes = [i32, C.POINTER(d)]
+        L.sal_direct_sum_noalloc.argtypes = [vp, vp, vp, vp, i32, vp, i32, vp, vp, vp]
         _lib = L
         return L
 
@@ -325,6 +326,22 @@ def fma_peak(precision=64) -> float:
     v = C.c_double()
     _check(lib().sal_fma_peak(int(precision), C.byref(v)))
     return v.value
+
+
+NOALLOC_MAX_TARGETS = (1 << 18) // 2   # SAL_NOALLOC_SCRATCH_DOUBLES / 2
+
+
+def direct_sum_noalloc(xs, ys, zs, w, targets, out_x, out_y, stream=None):
+    """direct_sum through sal_direct_sum_noalloc: the library allocates no
+    device memory (partial sums go to a fixed 2 MiB array of its own), so the
+    caller passes preallocated outputs.  Calls that overlap on the GPU race."""
+    import torch
+    st = stream if stream is not None else torch.cuda.current_stream(xs.device).cuda_stream
+    _check(lib().sal_direct_sum_noalloc(C.c_void_p(xs.data_ptr()), C.c_void_p(ys.data_ptr()),
+                                        C.c_void_p(zs.data_ptr()), C.c_void_p(w.data_ptr()), xs.numel(),
+                                        C.c_void_p(targets.data_ptr()), targets.numel(),
+                                        C.c_void_p(out_x.data_ptr()), C.c_void_p(out_y.data_ptr()), C.c_void_p(st)))
+    return out_x, out_y
 
 
 def direct_sum(xs, ys, zs, w, targets, stream=None):
