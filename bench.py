@@ -1,13 +1,16 @@
 """Benchmark of the B200 SAL-gradient treecode.
 
-One step = one solve of the SAL gradient (both components at every cell) of
-the field batch on a device-resident grid: the code.f90 path (dual tree
-traversal) on the 2,313,486-cell MPAS-like synthetic grid, d = 8, theta = 0.7,
-leaves < 200 points.  Inputs are seeded synthetic stand-ins of the reference's
-MPAS CSVs (not distributed with it).
+One step = one solve of the SAL gradient (both components at every cell) for
+the step's batch of SSH fields on a device-resident grid: the code.f90 path
+(dual tree traversal) on the 2,313,486-cell MPAS-like synthetic grid, d = 8,
+theta = 0.7, leaves < 200 points.  Inputs are seeded synthetic stand-ins for
+the reference's MPAS CSVs (not distributed with it).
 
-  python bench.py [--gpus N --steps K --warmup W] [--form ref|accurate] [--impl reference]
+  python bench.py [--gpus N --steps K --warmup W] [--form mixed|ref|accurate] [--fields F]
+  python bench.py --impl reference          # the CPU oracle port, same metric
 
+Default: the batched mixed-precision form, 64 fields per step (cfg3); the plain
+FP64 form of the same grid is timed in the same run and reported beside it.
 Multi-GPU runs are independent replicas (one grid per GPU, no collective in
 the solve): value = cells * fields * steps * world / max-over-ranks time.
 """
@@ -37,15 +40,23 @@ def _args():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--form", default="ref", choices=["ref", "accurate"])
-    ap.add_argument("--config", default="cfg2")
+    ap.add_argument("--form", default="mixed", choices=["ref", "accurate", "mixed"])
+    ap.add_argument("--fields", type=int, default=None)
+    ap.add_argument("--config", default=None)
     ap.add_argument("--degree", type=int, default=8)
     ap.add_argument("--thresh", type=int, default=200)
     ap.add_argument("--theta", type=float, default=0.7)
     ap.add_argument("--targets", type=int, default=10000)
+    ap.add_argument("--check-fields", type=int, default=4)
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--no-cpu", action="store_true")
-    return ap.parse_args()
+    ap.add_argument("--no-fp64", action="store_true")
+    a = ap.parse_args()
+    if a.fields is None:
+        a.fields = 64 if a.form == "mixed" else 1
+    if a.config is None:
+        a.config = "cfg3" if a.fields > 1 else "cfg2"
+    return a
 
 
 class Clocks:
@@ -93,14 +104,16 @@ def make_problem(args, device):
     from salgpu import synth
     t0 = time.perf_counter()
     g = synth.config_grid(args.config, device=device)
-    h = synth.config_ssh(args.config, g, nfields=1, device=device)
+    h = synth.config_ssh(args.config, g, nfields=args.fields, device=device)
     return g, h, time.perf_counter() - t0
 
 
 def cpu_baseline(args, g, h, sample_seconds):
     """The oracle (a line-faithful C restatement of the reference) on a random
     seeded sample of the interaction list with all host threads; the full
-    solve time is extrapolated by the sampled fraction of the list."""
+    one-field solve time is extrapolated by the sampled fraction of the list.
+    The reference solves one field per call, so its evals/s is the same for
+    any number of fields."""
     from oracle import oracle as O
     cores = os.cpu_count() or 1
     t0 = time.perf_counter()
@@ -109,7 +122,6 @@ def cpu_baseline(args, g, h, sample_seconds):
     setup = time.perf_counter() - t0
     pairs_all, macs_all = O.dtt_work(ot, L, args.degree)
     rng = np.random.default_rng(1234)
-    # pick the sample size from a short calibration run
     frac = 0.002
     while True:
         sel = np.sort(rng.choice(len(L), max(1, int(frac * len(L))), replace=False))
@@ -124,24 +136,32 @@ def cpu_baseline(args, g, h, sample_seconds):
     f_list = len(sel) / len(L)
     t_full = dt / f_list
     return {"value": g.n / t_full, "unit": "evals/s", "cores": cores, "kind": "port",
-            "sample": f"{len(sel)} of {len(L)} DTT interactions ({100 * f_list:.2f}%, seeded uniform; "
+            "sample": f"one field: {len(sel)} of {len(L)} DTT interactions ({100 * f_list:.2f}%, seeded uniform; "
                       f"{100 * f_work:.2f}% of pair+MAC work), {dt:.1f} s on {cores} threads, "
                       f"full solve extrapolated to {t_full:.1f} s; host setup {setup:.1f} s",
             "extrapolated_solve_s": t_full}
+
+
+def workload_name(args, n):
+    form = {"ref": "plain FP64 (reference operation order)", "accurate": "FP64 accurate form",
+            "mixed": "batched mixed precision: FP32 kernel tiles, TF32 3-pass tensor-core contractions, "
+                     "FP64 self pairs"}[args.form]
+    return (f"{args.config}: {n} cells x {args.fields} SSH fields, dual tree traversal (code.f90 fast_sum), "
+            f"d={args.degree}, theta={args.theta}, leaf<{args.thresh}; {form}")
 
 
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
+    args.fields = 1
     g, h, _ = make_problem(args, "cuda" if _cuda() else "cpu")
     cb = cpu_baseline(args, g, h[0], args.cpu_seconds)
     line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": "evals/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * cb["extrapolated_solve_s"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic: seeded Fibonacci ocean grid + spherical-harmonic SSH",
-            "config": {"workload": f"{args.config}: {g.n} cells, dual tree traversal (code.f90 fast_sum), "
-                                   f"d={args.degree}, theta={args.theta}, leaf<{args.thresh}, 1 field",
+            "config": {"workload": workload_name(args, g.n) + " (reference algorithm, one field per call)",
                        "cells": g.n, "fields": 1},
             "cpu_baseline": cb,
             "e2e": {"value": cb["value"], "unit": "evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -154,6 +174,18 @@ def _cuda():
         return torch.cuda.is_available()
     except Exception:
         return False
+
+
+def time_solves(torch, grid, ssh, form, out, steps, flush, stream):
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    for k in range(steps):
+        flush.fill_(float(k))                 # evicts L2 between timed solves
+        starts[k].record(stream)
+        grid.solve(ssh, form=form, out=out)
+        ends[k].record(stream)
+    torch.cuda.synchronize()
+    return np.array([s.elapsed_time(e) for s, e in zip(starts, ends)])
 
 
 def main():
@@ -172,16 +204,17 @@ def main():
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=600))
     dev = torch.device("cuda", local)
-    form = {"ref": S.FORM_REF, "accurate": S.FORM_ACCURATE}[args.form]
+    form = {"ref": S.FORM_REF, "accurate": S.FORM_ACCURATE, "mixed": S.FORM_MIXED}[args.form]
+    F = args.fields
 
     g, h, t_gen = make_problem(args, dev)
     t0 = time.perf_counter()
     tree = S.tree_traverse(g.xs, g.ys, g.zs, g.n, args.thresh)
     inter = S.dual_tree_traversal(tree, args.theta, args.thresh)
     t_lists = time.perf_counter() - t0
-    grid = S.Grid(tree, g.xs, g.ys, g.zs, g.areas, args.degree, S.MODE_DTT, inter, device=local)
+    grid = S.Grid(tree, g.xs, g.ys, g.zs, g.areas, args.degree, S.MODE_DTT, inter, device=local, max_fields=F)
     st = grid.stats()
-    ssh = torch.tensor(h[0], device=dev)
+    ssh = torch.tensor(h, device=dev)                      # (F, N), resident before timing
     ox = torch.empty_like(ssh)
     oy = torch.empty_like(ssh)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)   # > 126 MB L2
@@ -192,24 +225,16 @@ def main():
     torch.cuda.synchronize()
     grid.sync()
 
-    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     clk = Clocks(local)
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
     clk.start()
-    for k in range(args.steps):
-        flush.fill_(float(k))                 # evicts L2 between timed solves
-        starts[k].record(stream)
-        grid.solve(ssh, form=form, out=(ox, oy))
-        ends[k].record(stream)
-    torch.cuda.synchronize()
+    per = time_solves(torch, grid, ssh, form, (ox, oy), args.steps, flush, stream)
     clocks = clk.stop()
     if world > 1:
         dist.barrier()
     grid.sync()
-    per = np.array([s.elapsed_time(e) for s, e in zip(starts, ends)])
     total_ms = float(per.sum())
     if world > 1:
         t = torch.tensor([total_ms], device=dev)
@@ -222,66 +247,97 @@ def main():
         flush.fill_(float(k))
         grid.solve(ssh, form=form, out=(ox, oy))
     phase, nsol = grid.timing(0)
-    leaf_ms = phase[2] / nsol
-    proxy_ms = phase[1] / nsol
-    up_ms = phase[0] / nsol
+    up_ms, proxy_ms, leaf_ms = (phase[i] / nsol for i in range(3))
+    if form == S.FORM_MIXED:                     # one timing record per field block
+        nblk = (F + 63) // 64 if F > 32 else 1
+        up_ms, proxy_ms, leaf_ms = up_ms * nblk, proxy_ms * nblk, leaf_ms * nblk
 
     # ---- accuracy vs the FP64 direct sum on sampled targets
     tg = np.sort(np.random.default_rng(99).choice(g.n, min(args.targets, g.n), replace=False)).astype(np.int32)
     T = lambda a: torch.tensor(a, device=dev)
-    dx, dy = S.direct_sum(T(g.xs), T(g.ys), T(g.zs), T(g.areas * h[0]), T(tg))
     tgt = torch.tensor(tg, device=dev, dtype=torch.long)
-    ex, ey = ox[tgt] - dx, oy[tgt] - dy
-    rel = float(torch.sqrt((ex * ex + ey * ey).sum() / (dx * dx + dy * dy).sum()))
-    mx = float(torch.sqrt(ex * ex + ey * ey).max() / torch.sqrt(dx * dx + dy * dy).max())
+    rels, mxs = [], []
+    for f in range(min(args.check_fields, F)):
+        dx, dy = S.direct_sum(T(g.xs), T(g.ys), T(g.zs), T(g.areas * h[f]), T(tg))
+        ex, ey = ox[f][tgt] - dx, oy[f][tgt] - dy
+        rels.append(float(torch.sqrt((ex * ex + ey * ey).sum() / (dx * dx + dy * dy).sum())))
+        mxs.append(float(torch.sqrt(ex * ex + ey * ey).max() / torch.sqrt(dx * dx + dy * dy).max()))
 
-    # ---- end to end through the host-buffer C-ABI entry point (fast_sum)
-    h_ssh = torch.tensor(h[0]).pin_memory().numpy()
-    h_x = torch.zeros(g.n, dtype=torch.float64).pin_memory().numpy()
-    h_y = torch.zeros(g.n, dtype=torch.float64).pin_memory().numpy()
-    for _ in range(2):
-        grid.fast_sum_host(h_ssh, h_x, h_y, form)
+    # ---- plain FP64 form of the same grid, for the batched-vs-plain ratio
+    plain = None
+    if form == S.FORM_MIXED and not args.no_fp64:
+        s1 = ssh[:1].contiguous()
+        o1 = (torch.empty_like(s1), torch.empty_like(s1))
+        for _ in range(2):
+            grid.solve(s1, form=S.FORM_REF, out=o1)
+        pp = time_solves(torch, grid, s1, S.FORM_REF, o1, 3, flush, stream)
+        plain = g.n / (float(pp.mean()) * 1e-3)
+
+    # ---- end to end through the host-buffer C ABI (pinned buffers)
+    h_ssh = torch.tensor(h).pin_memory()
+    h_x = torch.empty_like(h_ssh).pin_memory()
+    h_y = torch.empty_like(h_ssh).pin_memory()
+    hs, hx, hy = h_ssh.numpy(), h_x.numpy(), h_y.numpy()
+    grid.solve_host(hs, hx, hy, form)
     e2e_t = []
-    for _ in range(max(3, args.steps // 2)):
+    for _ in range(max(3, args.steps // 3)):
         t1 = time.perf_counter()
-        grid.fast_sum_host(h_ssh, h_x, h_y, form)
+        grid.solve_host(hs, hx, hy, form)
         e2e_t.append(time.perf_counter() - t1)
-    e2e_val = g.n / float(np.mean(e2e_t))
+    e2e_val = g.n * F / float(np.mean(e2e_t))
 
-    peak64 = S.fma_peak(64)
-    leaf_flops = FLOPS_PER_PAIR * (st["pairs_pp"] + st["pairs_pc"]) + 2 * FLOPS_PER_MAC * st["macs_down"]
-    achieved = leaf_flops / (leaf_ms * 1e-3) / 1e12
-    total_flops = (FLOPS_PER_PAIR * (st["pairs_pp"] + st["pairs_pc"] + st["pairs_cp"] + st["pairs_cc"])
-                   + FLOPS_PER_MAC * (st["macs_up"] + 2 * st["macs_down"]))
+    # ---- roofline of the dominant kernel (the leaf pass)
+    if form == S.FORM_MIXED:
+        peaks = {}
+        try:
+            peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        except (OSError, ValueError):
+            pass
+        bf16 = peaks.get("bf16_tflops", 1590.0)
+        peak = bf16 / 2.0          # dense TF32 = half the bf16 rate
+        leaf_flops = 4.0 * F * (st["pairs_pp"] + st["pairs_pc"] + 3.0 * st["macs_down"])
+        achieved = leaf_flops / (leaf_ms * 1e-3) / 1e12
+        roof = {"bound": "tensor", "kernel": "mix_kernel<leaf> (PP+PC kernel tiles, DOWN interpolation)",
+                "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                "peak_source": ("TF32 dense = bf16_tflops/2 of measured" if "bf16_tflops" in peaks else
+                                "TF32 dense = 1.59 PFLOP/s bf16 fallback / 2"),
+                "flops_counted": "algorithmic 4*F per pair (2 components x FMA x F fields); the TF32 3-pass "
+                                 "split executes 3x these on the tensor cores",
+                "traffic": None, "leaf_ms": leaf_ms, "proxy_ms": proxy_ms, "prep_upward_ms": up_ms}
+    else:
+        peak64 = S.fma_peak(64)
+        leaf_flops = FLOPS_PER_PAIR * (st["pairs_pp"] + st["pairs_pc"]) + 2 * FLOPS_PER_MAC * st["macs_down"]
+        achieved = leaf_flops / (leaf_ms * 1e-3) / 1e12
+        roof = {"bound": "fp64", "kernel": "eval_kernel<leaf> (PP+PC pairs + DOWN interpolation)",
+                "achieved": achieved, "peak": peak64, "unit": "TFLOP/s", "frac": achieved / peak64,
+                "peak_source": "sal_fma_peak(64) on this GPU (FP64 FMA pipe; MEASURED_PEAKS.json has no FP64 figure)",
+                "traffic": None, "leaf_ms": leaf_ms, "proxy_ms": proxy_ms, "prep_upward_ms": up_ms}
 
     cb = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cb = cpu_baseline(args, g, h[0], args.cpu_seconds)
 
     if rank == 0:
-        value = g.n * args.steps * world / (total_ms * 1e-3)
+        value = g.n * F * args.steps * world / (total_ms * 1e-3)
         line = {
             "metric": METRIC, "value": value, "unit": "evals/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32/tf32 (fp64 self pairs)" if form == S.FORM_MIXED else "f64",
             "data": "synthetic: seeded Fibonacci ocean grid + spherical-harmonic SSH (stand-in for the MPAS CSVs)",
-            "config": {"workload": f"{args.config}: {g.n} cells, dual tree traversal (code.f90 fast_sum), "
-                                   f"d={args.degree}, theta={args.theta}, leaf<{args.thresh}, 1 field, "
-                                   f"{args.form} FP64 form", "cells": g.n, "fields": 1, "form": args.form,
+            "config": {"workload": workload_name(args, g.n), "cells": g.n, "fields": F, "form": args.form,
                        "parallelism": f"replicas x{world}", "l2": "flushed (256 MB write) between timed solves"},
             "latency_ms": {"p50": float(np.percentile(per, 50)), "p99": float(np.percentile(per, 99))},
-            "accuracy": {"rel_l2_vs_fp64_direct": rel, "max_err_over_max_ref": mx, "targets": len(tg)},
-            "roofline": {"bound": "fp64", "kernel": "eval_kernel<leaf> (PP+PC pairs + DOWN interpolation)",
-                         "achieved": achieved, "peak": peak64, "unit": "TFLOP/s", "frac": achieved / peak64,
-                         "peak_source": "sal_fma_peak(64) on this GPU (FP64 FMA pipe; MEASURED_PEAKS.json has no FP64 figure)",
-                         "traffic": None, "leaf_ms": leaf_ms, "proxy_ms": proxy_ms, "prep_upward_ms": up_ms,
-                         "algorithmic_tflop_per_solve": total_flops / 1e12},
+            "accuracy": {"rel_l2_vs_fp64_direct_max": max(rels), "rel_l2_vs_fp64_direct_mean": float(np.mean(rels)),
+                         "max_err_over_max_ref": max(mxs), "fields_checked": len(rels), "targets": len(tg)},
+            "plain_fp64": None if plain is None else {"value": plain, "unit": "evals/s",
+                                                      "batched_over_plain": value / world / plain},
+            "roofline": roof,
             "work": {k: st[k] for k in ("pairs_pp", "pairs_pc", "pairs_cp", "pairs_cc", "macs_up", "macs_down")},
             "setup_s": {"grid_generation": t_gen, "tree_and_lists": t_lists, "plan_and_upload": st["setup_seconds"]},
-            "e2e": {"value": e2e_val, "unit": "evals/s", "h2d_bytes_per_step": 8 * g.n,
-                    "d2h_bytes_per_step": 16 * g.n, "api": "sal_fast_sum_host (host buffers)"},
+            "e2e": {"value": e2e_val, "unit": "evals/s", "h2d_bytes_per_step": 8 * g.n * F,
+                    "d2h_bytes_per_step": 16 * g.n * F, "api": "sal_solve_host (pinned host buffers)"},
             "clocks": clocks,
-            "gpu_launches": 6 * args.steps,
+            "gpu_launches": 6 * args.steps * (((F + 63) // 64) if F > 32 else 1) if form == S.FORM_MIXED else 6 * args.steps,
         }
         if cb:
             line["cpu_baseline"] = cb

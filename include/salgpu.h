@@ -155,6 +155,12 @@ int sal_grid_destroy(sal_grid *g);
 int sal_solve(sal_grid *g, const double *ssh, int32_t nfields, int64_t ld_ssh, double *out_x, double *out_y,
               int64_t ld_out, int32_t form, void *stream);
 
+/* sal_solve on host buffers: copies the fields to the device, solves, copies
+ * both components back and waits (outputs overwritten).  Device staging is
+ * allocated on the first call and kept by the grid. */
+int sal_solve_host(sal_grid *g, const double *ssh, int32_t nfields, int64_t ld_ssh, double *out_x, double *out_y,
+                   int64_t ld_out, int32_t form);
+
 /* fast_sum, fast_sum_module.f90:291-332: adds the SAL gradient of one field
  * into host arrays sal_longrad/sal_latgrad (intent(inout)).  The grid must be
  * SAL_MODE_DTT.  form as in sal_solve. */

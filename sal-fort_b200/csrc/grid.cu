@@ -10,6 +10,7 @@
 
 #include "../../include/salgpu.h"
 #include "kernels.cuh"
+#include "mixed.cuh"
 #include "sal_internal.hpp"
 
 namespace sal {
@@ -53,8 +54,17 @@ struct GridImpl {
     double *src_nodes = nullptr;
     double *up_partial = nullptr;
     int *err = nullptr;
+    // batched mixed-precision form (allocated on its first solve)
+    int FT = 0;                       // fields per block: 32 or 64
+    float *wF = nullptr, *phiF = nullptr, *mix_up_partial = nullptr, *mix_proxy_partial = nullptr;
+    MixGroup *mix_leaf_groups = nullptr, *mix_proxy_groups = nullptr, *mix_up_groups = nullptr;
+    Item *mix_leaf_items = nullptr, *mix_proxy_items = nullptr;
+    double *tgt_nodes = nullptr;
+    int64_t mix_bytes = 0;
     // staging for the *_host entry points
     double *h_ssh = nullptr, *h_ox = nullptr, *h_oy = nullptr;  // device
+    double *hb_ssh = nullptr, *hb_ox = nullptr, *hb_oy = nullptr;  // device, batched
+    int hb_fields = 0;
     double *h_w = nullptr;                                        // device, P*npanels
     std::vector<void *> allocs;
     std::mutex mu;
@@ -202,6 +212,7 @@ extern "C" int sal_grid_create(const sal_tree *t_, const sal_grid_desc *d, sal_g
     TRY(dupload(g, &g.up_units, pl.up_units.data(), pl.up_units.size()));
     TRY(dupload(g, &g.up_unit_beg, pl.up_unit_beg.data(), pl.up_unit_beg.size()));
     TRY(dupload(g, &g.src_nodes, pl.src_nodes.data(), pl.src_nodes.size()));
+    TRY(dupload(g, &g.tgt_nodes, pl.tgt_nodes.data(), pl.tgt_nodes.size()));
     TRY(dalloc(g, &g.up_partial, (size_t)g.nup * P));
     TRY(dalloc(g, &g.err, 1));
     CK(cudaMemset(g.err, 0, sizeof(int)));
@@ -309,15 +320,111 @@ static void solve_fp64(GridImpl &g, const double *ssh, double *ox, double *oy, i
     }
 }
 
+// Device buffers of the batched form, sized for blocks of FT fields.
+static int ensure_mixed(GridImpl &g, int FT) {
+    if (g.FT == FT) return SAL_OK;
+    if (g.FT != 0) return set_error(SAL_EINVAL, "a grid's batched buffers are sized for one field block width");
+    const Plan &pl = g.plan;
+    const size_t P = (size_t)pl.P, n = (size_t)pl.n;
+    const int64_t before = g.bytes;
+    int rc = SAL_OK;
+    if (!rc) rc = dalloc(g, &g.wF, (n + (size_t)g.nsrc * P) * FT);
+    if (!rc) rc = dalloc(g, &g.phiF, (size_t)g.ntgt * 3 * P * FT);
+    if (!rc) rc = dalloc(g, &g.mix_up_partial, (size_t)g.nup * P * FT);
+    if (!rc) rc = dalloc(g, &g.mix_proxy_partial, (size_t)g.nproxy_units * 3 * P * FT);
+    if (!rc) rc = dupload(g, &g.mix_leaf_groups, pl.mix_leaf_groups.data(), pl.mix_leaf_groups.size());
+    if (!rc) rc = dupload(g, &g.mix_leaf_items, pl.mix_leaf_items.data(), pl.mix_leaf_items.size());
+    if (!rc) rc = dupload(g, &g.mix_proxy_groups, pl.mix_proxy_groups.data(), pl.mix_proxy_groups.size());
+    if (!rc) rc = dupload(g, &g.mix_proxy_items, pl.mix_proxy_items.data(), pl.mix_proxy_items.size());
+    if (!rc) rc = dupload(g, &g.mix_up_groups, pl.mix_up_groups.data(), pl.mix_up_groups.size());
+    if (rc) return rc;
+    g.FT = FT;
+    g.mix_bytes = g.bytes - before;
+    return SAL_OK;
+}
+
+// One block of up to FT fields in the batched form: per-field weights, upward
+// pass, proxy potentials, leaf pass (six launches).
+static void solve_mixed_block(GridImpl &g, const double *ssh, int64_t ld_ssh, int f0, int nf, double *ox, double *oy,
+                              int64_t ld_out, cudaStream_t st) {
+    const Plan &pl = g.plan;
+    const int n = pl.n, P = pl.P, FT = g.FT;
+    if (g.timing) cudaEventRecord(g.ev[0], st);
+    mix::launch_prep_mix(g.area, ssh, ld_ssh, g.perm, n, f0, nf, FT, g.wF, st);
+    mix::MixArgs a{};
+    a.pool = g.pool;
+    a.wF = g.wF;
+    a.phiF = g.phiF;
+    a.xieta = g.xieta;
+    a.d = pl.d;
+    a.P = P;
+    a.perm = g.perm;
+    a.area = g.area;
+    a.ssh = ssh;
+    a.ld_ssh = ld_ssh;
+    a.out_x = ox;
+    a.out_y = oy;
+    a.ld_out = ld_out;
+    a.f0 = f0;
+    a.nf = nf;
+    if (!pl.mix_up_groups.empty()) {
+        mix::MixArgs u = a;
+        u.groups = g.mix_up_groups;
+        u.tgt_nodes = g.src_nodes;
+        u.partial = g.mix_up_partial;
+        mix::launch_mix(2, FT, u, (int)pl.mix_up_groups.size(), st);
+        mix::launch_finalize_mix(g.up_unit_beg, g.mix_up_partial, g.nsrc, P, FT, g.wF + (size_t)n * FT, st);
+    }
+    if (g.timing) cudaEventRecord(g.ev[1], st);
+    if (!pl.mix_proxy_groups.empty()) {
+        mix::MixArgs q = a;
+        q.groups = g.mix_proxy_groups;
+        q.items = g.mix_proxy_items;
+        q.tgt = g.tgt_proxy;
+        q.partial = g.mix_proxy_partial;
+        mix::launch_mix(1, FT, q, (int)pl.mix_proxy_groups.size(), st);
+        mix::launch_finalize_mix(g.proxy_unit_beg, g.mix_proxy_partial, g.ntgt, 3 * P, FT, g.phiF, st);
+    }
+    if (g.timing) cudaEventRecord(g.ev[2], st);
+    a.groups = g.mix_leaf_groups;
+    a.items = g.mix_leaf_items;
+    a.tgt = g.pool;
+    a.tgt_nodes = g.tgt_nodes;
+    mix::launch_mix(0, FT, a, (int)pl.mix_leaf_groups.size(), st);
+    if (g.timing) {
+        cudaEventRecord(g.ev[3], st);
+        cudaEventSynchronize(g.ev[3]);
+        float t01 = 0, t12 = 0, t23 = 0;
+        cudaEventElapsedTime(&t01, g.ev[0], g.ev[1]);
+        cudaEventElapsedTime(&t12, g.ev[1], g.ev[2]);
+        cudaEventElapsedTime(&t23, g.ev[2], g.ev[3]);
+        g.phase_ms[0] += t01;
+        g.phase_ms[1] += t12;
+        g.phase_ms[2] += t23;
+        g.phase_ms[3] += t01 + t12 + t23;
+        g.phase_solves += 1;
+    }
+}
+
 extern "C" int sal_solve(sal_grid *G, const double *ssh, int32_t nf, int64_t ld_ssh, double *ox, double *oy,
                          int64_t ld_out, int32_t form, void *stream) {
     if (!G || !ssh || !ox || !oy) return set_error(SAL_EINVAL, "null argument");
     GridImpl &g = G->g;
     if (nf < 1) return set_error(SAL_EINVAL, "nfields must be >= 1");
     if (nf > 1 && (ld_ssh < g.plan.n || ld_out < g.plan.n)) return set_error(SAL_EINVAL, "leading dimension < point_count");
-    if (form != SAL_FORM_REF && form != SAL_FORM_ACCURATE) return set_error(SAL_EINVAL, "unsupported form");
+    if (form != SAL_FORM_REF && form != SAL_FORM_ACCURATE && form != SAL_FORM_MIXED)
+        return set_error(SAL_EINVAL, "unsupported form");
     CK(cudaSetDevice(g.dev));
     cudaStream_t st = (cudaStream_t)stream;  // NULL: the CUDA default stream
+    if (form == SAL_FORM_MIXED) {
+        if (g.plan.mode != SAL_MODE_DTT) return set_error(SAL_EINVAL, "the batched form needs a SAL_MODE_DTT grid");
+        const int FT = g.FT ? g.FT : (nf <= 32 ? 32 : 64);
+        int rc = ensure_mixed(g, FT);
+        if (rc) return rc;
+        for (int f0 = 0; f0 < nf; f0 += FT) solve_mixed_block(g, ssh, ld_ssh, f0, nf, ox, oy, ld_out, st);
+        CK(cudaGetLastError());
+        return SAL_OK;
+    }
     for (int f = 0; f < nf; ++f)
         solve_fp64(g, ssh + (size_t)f * ld_ssh, ox + (size_t)f * ld_out, oy + (size_t)f * ld_out,
                    g.plan.mode == SAL_MODE_DTT ? form : SAL_FORM_REF, 7, true, st);
@@ -383,6 +490,36 @@ static int add_back(GridImpl &g, double *hx, double *hy) {
         hy[i] += ty[i];
     }
     return SAL_OK;
+}
+
+extern "C" int sal_solve_host(sal_grid *G, const double *ssh, int32_t nf, int64_t ld_ssh, double *ox, double *oy,
+                              int64_t ld_out, int32_t form) {
+    if (!G || !ssh || !ox || !oy) return set_error(SAL_EINVAL, "null argument");
+    GridImpl &g = G->g;
+    const int64_t n = g.plan.n;
+    if (nf < 1) return set_error(SAL_EINVAL, "nfields must be >= 1");
+    if (nf > 1 && (ld_ssh < n || ld_out < n)) return set_error(SAL_EINVAL, "leading dimension < point_count");
+    std::lock_guard<std::mutex> lk(g.mu);
+    CK(cudaSetDevice(g.dev));
+    if (g.hb_fields < nf) {
+        int rc = dalloc(g, &g.hb_ssh, (size_t)n * nf);
+        if (!rc) rc = dalloc(g, &g.hb_ox, (size_t)n * nf);
+        if (!rc) rc = dalloc(g, &g.hb_oy, (size_t)n * nf);
+        if (rc) return rc;
+        g.hb_fields = nf;
+    }
+    for (int f = 0; f < nf; ++f)
+        CK(cudaMemcpyAsync(g.hb_ssh + (size_t)f * n, ssh + (size_t)f * ld_ssh, (size_t)n * 8, cudaMemcpyHostToDevice,
+                           g.stream));
+    int rc = sal_solve(G, g.hb_ssh, nf, n, g.hb_ox, g.hb_oy, n, form, g.stream);
+    if (rc) return rc;
+    for (int f = 0; f < nf; ++f) {
+        CK(cudaMemcpyAsync(ox + (size_t)f * ld_out, g.hb_ox + (size_t)f * n, (size_t)n * 8, cudaMemcpyDeviceToHost,
+                           g.stream));
+        CK(cudaMemcpyAsync(oy + (size_t)f * ld_out, g.hb_oy + (size_t)f * n, (size_t)n * 8, cudaMemcpyDeviceToHost,
+                           g.stream));
+    }
+    return finish(g, g.stream);
 }
 
 extern "C" int sal_fast_sum_host(sal_grid *G, const double *ssh, double *lon, double *lat, int32_t form) {

@@ -1,0 +1,39 @@
+// Launch interface of the batched mixed-precision kernels (mixed.cu).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "sal_internal.hpp"
+
+namespace sal {
+namespace mix {
+
+struct MixArgs {
+    const double4 *pool;      // FP64 source coordinates (points, then source proxies)
+    const float *wF;          // per-field source rows: (n + nsrc*P) x FT
+    const float *phiF;        // per-field Cartesian potentials: ntgt x 3P x FT
+    const MixGroup *groups;
+    const Item *items;
+    const double4 *tgt;       // target coordinates: pool (leaf) or target proxies (proxy pass)
+    const double2 *xieta;     // per pool position
+    const double *tgt_nodes;  // 2(d+1) Chebyshev nodes per slot (target slots; source slots for the upward pass)
+    int d, P;
+    const int32_t *perm;      // leaf epilogue: pool position -> caller index
+    const double *area;       // per pool position
+    const double *ssh;        // caller's fields (column f at ssh + f*ld_ssh)
+    int64_t ld_ssh;
+    double *out_x, *out_y;    // caller's outputs (column f at + f*ld_out)
+    int64_t ld_out;
+    float *partial;           // proxy / upward: per-unit partial sums
+    int f0, nf;               // first field of this block, total fields
+};
+
+void launch_mix(int kind, int FT, const MixArgs &a, int ngroups, cudaStream_t st);
+void launch_prep_mix(const double *area, const double *ssh, int64_t ld, const int32_t *perm, int n, int f0, int nf,
+                     int FT, float *wF, cudaStream_t st);
+void launch_finalize_mix(const int32_t *unit_beg, const float *partial, int nslots, int rows_per_slot, int FT,
+                         float *dst, cudaStream_t st);
+size_t mix_smem_bytes();
+
+}  // namespace mix
+}  // namespace sal

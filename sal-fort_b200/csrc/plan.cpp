@@ -286,6 +286,63 @@ bool plan_build(const Tree &t, int d, int mode, const int32_t *list, int64_t nli
         std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) { return ucost[a] > ucost[b]; });
         for (int32_t u : ord) pl->proxy_groups.push_back(units[u]);
     }
+    // ---------------------------------------------------------------- batched-form groups
+    // Same work as above, re-cut for the tensor-core kernels: items of at most
+    // kMixStage sources, groups of at most kMixRows targets, and a local
+    // coordinate origin per group (the panel centre) so the FP32 kernel tiles
+    // see small coordinate differences.
+    {
+        auto rechunk = [&](const std::vector<Item> &src, int32_t ib, int32_t ie, std::vector<Item> &dst) {
+            for (int32_t i = ib; i < ie; ++i) {
+                const Item &it = src[i];
+                if (it.kind == 2) {
+                    for (int r = 0; r < 3 * P; r += kMixStage)
+                        dst.push_back(Item{it.off, std::min(kMixStage, 3 * P - r), r, 2});
+                } else {
+                    for (int b = 0; b < it.cnt; b += kMixStage)
+                        dst.push_back(Item{it.off + b, std::min(kMixStage, it.cnt - b), it.mask, it.kind});
+                }
+            }
+        };
+        pl->mix_leaf_groups.clear();
+        pl->mix_leaf_items.clear();
+        if (dtt) {
+            for (const Group &g : pl->leaf_groups) {
+                int32_t ib = (int32_t)pl->mix_leaf_items.size();
+                rechunk(pl->leaf_items, g.ib, g.ie, pl->mix_leaf_items);
+                int32_t ie = (int32_t)pl->mix_leaf_items.size();
+                const int k = leaves[g.out];
+                for (int32_t r = 0; r < g.nt; r += kMixRows) {
+                    MixGroup m{};
+                    m.tgt = g.tgt + r; m.nt = std::min(kMixRows, g.nt - r); m.ib = ib; m.ie = ie; m.out = g.out;
+                    m.cx = t.cx[k]; m.cy = t.cy[k]; m.cz = t.cz[k];
+                    pl->mix_leaf_groups.push_back(m);
+                }
+            }
+            pl->mix_proxy_groups.clear();
+            pl->mix_proxy_items.clear();
+            for (const Group &g : pl->proxy_groups) {
+                int32_t ib = (int32_t)pl->mix_proxy_items.size();
+                rechunk(pl->proxy_items, g.ib, g.ie, pl->mix_proxy_items);
+                int32_t ie = (int32_t)pl->mix_proxy_items.size();
+                const int k = pl->tgt_slot_panel[g.tgt];
+                for (int32_t r = 0; r < P; r += kMixRows) {
+                    MixGroup m{};
+                    m.tgt = g.tgt; m.nt = std::min(kMixRows, P - r); m.ib = ib; m.ie = ie; m.out = g.out; m.row0 = r;
+                    m.cx = t.cx[k]; m.cy = t.cy[k]; m.cz = t.cz[k];
+                    pl->mix_proxy_groups.push_back(m);
+                }
+            }
+            pl->mix_up_groups.clear();
+            for (size_t u = 0; u < pl->up_units.size(); ++u)
+                for (int32_t r = 0; r < P; r += kMixRows) {
+                    MixGroup m{};
+                    m.tgt = pl->up_units[u].slot; m.nt = std::min(kMixRows, P - r); m.ib = pl->up_units[u].beg;
+                    m.ie = pl->up_units[u].end; m.out = (int32_t)u; m.row0 = r;
+                    pl->mix_up_groups.push_back(m);
+                }
+        }
+    }
     // ---------------------------------------------------------------- point data in pool order
     pl->pxi.resize(n); pl->peta.resize(n);
     for (int32_t p = 0; p < n; ++p) { pl->pxi[p] = t.xi[t.order[p]]; pl->peta[p] = t.eta[t.order[p]]; }

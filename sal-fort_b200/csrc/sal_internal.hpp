@@ -53,9 +53,10 @@ int assign_points_to_panels(const Tree &t, const double *xs, const double *ys, c
                             int32_t *points_panels, int32_t nlev);
 
 // ---------------------------------------------------------------- work plan
-// Item of a target group's work list.  kind 0: sources are pool entries
-// [off, off+cnt) (points or proxies); kind 1: a DOWN item, interpolation from
-// target slot `off`.  mask: word offset of the per-target bitmask (STT), or -1.
+// Item of a target group's work list.  kind 0 (PP) / 1 (PC): sources are pool
+// entries [off, off+cnt) (points / proxies); kind 2 (DOWN): interpolation from
+// the potentials of target slot `off`.  mask: word offset of the per-target
+// bitmask (STT), or -1.
 struct Item {
     int32_t off, cnt, mask, kind;
 };
@@ -70,6 +71,15 @@ struct Group {           // a set of targets with one work list
 
 struct UpUnit {          // upward-pass work unit
     int32_t slot, beg, end, panel;
+};
+
+// Target group of the batched (mixed-precision) kernels: at most 64 targets
+// (four 16-row tensor-core tiles) with a local coordinate origin (cx, cy, cz)
+// near them.  row0: first target row of the group within its panel (proxy
+// groups) or 0.
+struct MixGroup {
+    int32_t tgt, nt, ib, ie, out, row0, pad0, pad1;
+    double cx, cy, cz, pad2;
 };
 
 struct Plan {
@@ -94,6 +104,10 @@ struct Plan {
     std::vector<Group> leaf_groups;               // one per leaf with targets, sorted by cost
     std::vector<Item> leaf_items;
     std::vector<uint32_t> masks;                  // STT per-target bitmasks
+    // batched form: items of at most kMixStage sources (DOWN items: rows of
+    // a target slot's potentials, off = slot, cnt = rows, mask = first row)
+    std::vector<MixGroup> mix_leaf_groups, mix_proxy_groups, mix_up_groups;
+    std::vector<Item> mix_leaf_items, mix_proxy_items;
     double pairs[4] = {0, 0, 0, 0};               // PP, PC, CP, CC evaluations per field
     double macs_up = 0, macs_down = 0;
     int32_t max_nt = 0;
@@ -104,6 +118,8 @@ bool plan_build(const Tree &t, int d, int mode, const int32_t *list, int64_t nli
                 const int32_t *pp, int64_t npp, Plan *plan, std::string *err);
 
 constexpr int kMaxStage = 256;   // sources staged per item (items are split to fit)
-constexpr int kMaxDegree = 15;   // (d+1)^2 <= 256 proxies
+constexpr int kMixStage = 64;    // sources (or DOWN rows) staged per batched item
+constexpr int kMixRows = 64;     // targets per batched CTA
+constexpr int kMaxDegree = 14;   // a DOWN record (4(d+1)^2 + 2(d+1) doubles) fits one 8 KB stage
 
 }  // namespace sal

@@ -1,0 +1,66 @@
+"""GPU tests of the batched mixed-precision form (SAL_FORM_MIXED).
+
+Bars (rel-L2 over both components, per field):
+  * vs the FP64 accurate form (same algorithm):  <= 5e-6
+  * vs the FP64 direct sum (all cells):           <= 1e-5
+  * a field alone vs the same field in a batch:   identical (the tensor-core
+    columns of different fields never mix)
+"""
+import numpy as np
+import pytest
+
+from conftest import grid_and_ssh, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+
+def _torch():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    return torch
+
+
+def _grid(name, thresh, nfields, seed=11, degree=8):
+    import salgpu as S
+    g, hs = grid_and_ssh(name, nfields=nfields, seed=seed)
+    t = S.tree_traverse(g.xs, g.ys, g.zs, g.n, thresh)
+    L = S.dual_tree_traversal(t, 0.7, thresh)
+    return S, g, hs, S.Grid(t, g.xs, g.ys, g.zs, g.areas, degree, S.MODE_DTT, L, max_fields=nfields)
+
+
+@pytest.mark.parametrize("name,thresh", [("small_3000", 20), ("cfg0", 100)])
+def test_mixed_matches_fp64_accurate_and_direct_sum(name, thresh):
+    torch = _torch()
+    S, g, hs, grid = _grid(name, thresh, 5)
+    ssh = torch.tensor(hs, device="cuda")
+    mx, my = grid.solve(ssh, form=S.FORM_MIXED)
+    ax, ay = grid.solve(ssh, form=S.FORM_ACCURATE)
+    T = lambda a: torch.tensor(a, device="cuda")
+    tg = T(np.arange(g.n, dtype=np.int32))
+    torch.cuda.synchronize()
+    for f in range(5):
+        dx, dy = S.direct_sum(T(g.xs), T(g.ys), T(g.zs), T(g.areas * hs[f]), tg)
+        m = [v[f].cpu().numpy() for v in (mx, my, ax, ay)]
+        d = [dx.cpu().numpy(), dy.cpu().numpy()]
+        assert rel_l2(m[0], m[1], m[2], m[3]) <= 5e-6
+        assert rel_l2(m[0], m[1], d[0], d[1]) <= 1e-5
+
+
+def test_mixed_batch_invariance_and_field_blocks():
+    torch = _torch()
+    S, g, hs, grid = _grid("small_3000", 20, 70, seed=3)
+    ssh = torch.tensor(hs, device="cuda")
+    bx, by = grid.solve(ssh[:40], form=S.FORM_MIXED)          # one 64-field block
+    cx, cy = grid.solve(ssh, form=S.FORM_MIXED)               # two blocks (64 + 6)
+    torch.cuda.synchronize()
+    for f in (0, 17, 39):
+        ox, oy = grid.solve(ssh[f:f + 1], form=S.FORM_MIXED)  # the field alone
+        torch.cuda.synchronize()
+        assert torch.equal(ox[0], bx[f]) and torch.equal(oy[0], by[f])
+        assert torch.equal(ox[0], cx[f]) and torch.equal(oy[0], cy[f])
+    ax, ay = grid.solve(ssh[65:70], form=S.FORM_ACCURATE)
+    torch.cuda.synchronize()
+    for f in range(5):
+        assert rel_l2(cx[65 + f].cpu().numpy(), cy[65 + f].cpu().numpy(), ax[f].cpu().numpy(),
+                      ay[f].cpu().numpy()) <= 5e-6
