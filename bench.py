@@ -51,6 +51,9 @@ def _args():
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--serve-seconds", type=float, default=8.0)
+    ap.add_argument("--serve-rate", type=float, default=200.0)
+    ap.add_argument("--no-serve", action="store_true")
     a = ap.parse_args()
     if a.fields is None:
         a.fields = 64 if a.form == "mixed" else 1
@@ -166,6 +169,51 @@ def run_reference(args):
             "cpu_baseline": cb,
             "e2e": {"value": cb["value"], "unit": "evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def serving_run(args, S, torch, dev):
+    """The serving mix: four Fibonacci ocean grids (40,962 / 163,842 / 655,362
+    / 2,313,486 cells) resident under an HBM budget, Poisson arrivals at
+    args.serve_rate per second, each request 1-16 fields drawn from a pool of
+    seeded degree 1-128 fields of its grid (grid weights 0.4/0.3/0.2/0.1),
+    batched per grid as they arrive.  Returns latency percentiles, throughput
+    and the accuracy of sampled served results vs the FP64 direct sum."""
+    from salgpu import serve, synth
+    sizes = {"serve_40962": 40962, "serve_163842": 163842, "serve_655362": 655362, "serve_2313486": 2313486}
+    weights = {"serve_40962": 0.4, "serve_163842": 0.3, "serve_655362": 0.2, "serve_2313486": 0.1}
+    srv = serve.Server(60 << 30, max_batch=64, device=dev.index or 0)
+    pools, grids = {}, {}
+    for name in sizes:
+        g = synth.config_grid(name, device=dev)
+        pools[name] = synth.config_ssh("cfg3", g, nfields=16, seed=31, device=dev)
+        grids[name] = g
+        srv.register_grid(serve.GridSpec(name, g.xs, g.ys, g.zs, g.areas, args.degree, args.thresh, args.theta))
+    # admit every grid and warm its kernels before the clock starts
+    for name in sizes:
+        srv.submit(serve.Request(name, pools[name][:2]))
+    srv.run_until_idle()
+    t0 = time.perf_counter()
+    reqs = serve.run_workload(srv, pools, weights, args.serve_rate, args.serve_seconds, seed=7)
+    wall = time.perf_counter() - t0
+    out = serve.summarize(reqs, sizes, wall)
+    out.update({"rate_req_per_s": args.serve_rate, "seconds": args.serve_seconds, "max_batch_fields": 64,
+                "evictions": srv.evictions})
+    # accuracy of served results: first field of a few requests of each grid
+    T = lambda a: torch.tensor(a, device=dev)
+    errs = []
+    for name in sizes:
+        done = [q for q in reqs if q.grid == name and q.status == "done"][:2]
+        g = grids[name]
+        tg = np.sort(np.random.default_rng(5).choice(g.n, min(2000, g.n), replace=False)).astype(np.int32)
+        for q in done:
+            w = g.areas * q.ssh[0]
+            dx, dy = S.direct_sum(T(g.xs), T(g.ys), T(g.zs), T(w), T(tg))
+            dx, dy = dx.cpu().numpy(), dy.cpu().numpy()
+            ex, ey = q.out_x[0][tg] - dx, q.out_y[0][tg] - dy
+            errs.append(float(np.sqrt(np.sum(ex * ex + ey * ey) / np.sum(dx * dx + dy * dy))))
+    out["rel_l2_vs_fp64_direct_max"] = max(errs) if errs else None
+    srv.close()
+    return out
 
 
 def _cuda():
@@ -316,6 +364,11 @@ def main():
     cb = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cb = cpu_baseline(args, g, h[0], args.cpu_seconds)
+    served = None
+    if rank == 0 and world == 1 and form == S.FORM_MIXED and not args.no_serve:
+        del grid
+        torch.cuda.empty_cache()
+        served = serving_run(args, S, torch, dev)
 
     if rank == 0:
         value = g.n * F * args.steps * world / (total_ms * 1e-3)
@@ -341,6 +394,8 @@ def main():
         }
         if cb:
             line["cpu_baseline"] = cb
+        if served:
+            line["serving"] = served
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()

@@ -111,7 +111,7 @@ typedef struct {
     int64_t pc_count;
     const int32_t *pp_list;
     int64_t pp_count;
-    int32_t max_fields;  /* largest number of SSH fields one sal_solve call may carry (>= 1) */
+    int32_t max_fields;  /* fields per batched block: <= 32 sizes the batched buffers for 32, else 64 */
     int32_t device;      /* CUDA device ordinal */
 } sal_grid_desc;
 
@@ -122,6 +122,7 @@ typedef struct {
     double macs_up, macs_down;                       /* proxy multiply-adds per field per solve */
     int64_t device_bytes;                            /* resident device memory of the grid */
     double setup_seconds;                            /* plan build + upload */
+    int64_t mixed_bytes;                             /* device memory the batched form adds on its first solve */
 } sal_grid_stats;
 
 /* Flattens the tree and lists into device-resident arrays (once per grid). */

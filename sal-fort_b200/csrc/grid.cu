@@ -56,6 +56,7 @@ struct GridImpl {
     int *err = nullptr;
     // batched mixed-precision form (allocated on its first solve)
     int FT = 0;                       // fields per block: 32 or 64
+    int max_fields = 1;
     float *wF = nullptr, *phiF = nullptr, *mix_up_partial = nullptr, *mix_proxy_partial = nullptr;
     MixGroup *mix_leaf_groups = nullptr, *mix_proxy_groups = nullptr, *mix_up_groups = nullptr;
     Item *mix_leaf_items = nullptr, *mix_proxy_items = nullptr;
@@ -147,6 +148,7 @@ extern "C" int sal_grid_create(const sal_tree *t_, const sal_grid_desc *d, sal_g
     sal_grid *G = new sal_grid();
     GridImpl &g = G->g;
     g.dev = d->device;
+    g.max_fields = d->max_fields;
     std::string err;
     if (!plan_build(t, d->interp_degree, d->mode, d->list, d->list_count, d->pc_list, d->pc_count, d->pp_list,
                     d->pp_count, &g.plan, &err)) {
@@ -251,6 +253,15 @@ extern "C" int sal_grid_stats_get(const sal_grid *G, sal_grid_stats *s) {
     s->macs_down = pl.macs_down;
     s->device_bytes = g.bytes;
     s->setup_seconds = g.setup_seconds;
+    {
+        const int64_t FT = g.FT ? g.FT : (g.max_fields <= 32 ? 32 : 64), P = pl.P;
+        s->mixed_bytes = g.FT ? g.mix_bytes
+                              : 4 * FT * ((int64_t)pl.n + (int64_t)g.nsrc * P + 3 * P * (int64_t)g.ntgt + P * (int64_t)g.nup +
+                                          3 * P * (int64_t)g.nproxy_units) +
+                                    (int64_t)sizeof(MixGroup) * (int64_t)(pl.mix_leaf_groups.size() + pl.mix_proxy_groups.size() +
+                                                                          pl.mix_up_groups.size()) +
+                                    (int64_t)sizeof(Item) * (int64_t)(pl.mix_leaf_items.size() + pl.mix_proxy_items.size());
+    }
     return SAL_OK;
 }
 
@@ -418,7 +429,7 @@ extern "C" int sal_solve(sal_grid *G, const double *ssh, int32_t nf, int64_t ld_
     cudaStream_t st = (cudaStream_t)stream;  // NULL: the CUDA default stream
     if (form == SAL_FORM_MIXED) {
         if (g.plan.mode != SAL_MODE_DTT) return set_error(SAL_EINVAL, "the batched form needs a SAL_MODE_DTT grid");
-        const int FT = g.FT ? g.FT : (nf <= 32 ? 32 : 64);
+        const int FT = g.FT ? g.FT : (g.max_fields <= 32 ? 32 : 64);
         int rc = ensure_mixed(g, FT);
         if (rc) return rc;
         for (int f0 = 0; f0 < nf; f0 += FT) solve_mixed_block(g, ssh, ld_ssh, f0, nf, ox, oy, ld_out, st);

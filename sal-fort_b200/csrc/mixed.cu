@@ -32,7 +32,6 @@ using dev::smem_u32;
 
 constexpr int kThr = 128;          // 4 warps, one 16-row tile each
 constexpr int kS = kMixStage;      // K rows staged per item
-constexpr float kConsF = (float)dev::kCons;
 constexpr float kC1F = (float)dev::kC1;
 constexpr float kTwoC2F = (float)(2.0 * dev::kC2);
 
@@ -68,24 +67,28 @@ __device__ __forceinline__ int bofs(int k, int f) {
     return k * FT + ((((f >> 2) ^ ((k & 3) << 1))) << 2) + (f & 3);
 }
 
-// val of the kernel in FP32 from the chord d = s - t (antipode-stable form,
-// see dev::vstable).  mp == 0 (the self pair) gives a finite val.
-__device__ __forceinline__ float val32(float dx, float dy, float dz) {
-    const float mp = dx * dx + dy * dy + dz * dz;
-    float rq;
-    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(rq) : "f"(mp));
-    const float q = mp > 0.f ? mp * rq : 0.f;
-    const float d1 = q * mp + 1e-16f;
-    const float d2 = mp * (2.f + q) + 1e-16f;
-    const float num = kC1F * d2 - kTwoC2F * (1.f + q) * d1;
-    float r;
-    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(d1 * d2));
-    return kConsF * num * r;
+// val / kCons of the kernel in FP32 from the chord length squared mp = |s - t|^2
+// (the antipode-stable form of dev::vstable without its 1e-16 terms, which
+// only matter at s == t):  with r = 1/q and u = 1/(2 + q),
+//   kC1/q^3 - 2 kC2 (1 + q)/(q^2 (2 + q)) = r^2 (kC1 r - 2 kC2 (1 - u)).
+// mp == 0 (the self pair, added separately in FP64) gives 0.  The constant
+// kCons is folded into the per-field weights instead.
+__device__ __forceinline__ float val32(float mp) {
+    float r, u;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(mp));
+    const float q = mp * r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(u) : "f"(2.f + q));
+    const float inner = fmaf(kC1F, r, fmaf(kTwoC2F, u, -kTwoC2F));
+    const float v = inner * r * r;
+    return mp > 0.f ? v : 0.f;
 }
 
 struct Smem {
-    // B tiles, double-buffered: kS rows x FT floats each (sized for FT = 64)
+    // B tiles as copied, double-buffered: kS rows x FT floats each (sized for FT = 64)
     float B[2][kS * 64];
+    // the current item's B tile split into TF32 hi/lo, in mma fragment order:
+    // [k-step][n-tile][lane] = (b0 hi, b1 hi, b0 lo, b1 lo)
+    float4 Bf[(kS / 8) * 8 * 32];
     double4 raw[2][kS];              // staged FP64 source coordinates
     float4 loc[kS];                  // sources relative to the group's centre (FP32)
     float fx[kMixRows][kMaxDegree + 1];  // BLI bases: of targets (leaf DOWN) or sources (upward)
@@ -209,6 +212,8 @@ __global__ void __launch_bounds__(kThr) mix_kernel(MixArgs a) {
             if (tid < cnt) {
                 const double4 s = sm.raw[buf][tid];
                 sm.loc[tid] = make_float4((float)(s.x - G.cx), (float)(s.y - G.cy), (float)(s.z - G.cz), 0.f);
+            } else if (tid < ((cnt + 7) & ~7)) {
+                sm.loc[tid] = make_float4(4.f, 4.f, 4.f, 0.f);   // padding: finite tile entry, zero weight row
             }
         } else if (KIND == 0 && kind == 2) {
             if (sm.down_slot != off) {
@@ -235,6 +240,20 @@ __global__ void __launch_bounds__(kThr) mix_kernel(MixArgs a) {
                 for (int i = 0; i < n; ++i) sm.fe[tid - kS][i] = (float)f[i];
             }
         }
+        {
+            // split the staged B tile once for the whole CTA, in fragment order
+            const float *Bt = sm.B[buf];
+            const int nout = ((cnt + 7) >> 3) * NT * 32;
+            for (int o = tid; o < nout; o += kThr) {
+                const int ln = o & 31, j = (o >> 5) % NT, kk = (o >> 5) / NT;
+                const int kr = kk * 8 + (ln & 3), col = j * 8 + (ln >> 2);
+                uint32_t h0, l0, h1, l1;
+                split_tf32(Bt[bofs<FT>(kr, col)], h0, l0);
+                split_tf32(Bt[bofs<FT>(kr + 4, col)], h1, l1);
+                sm.Bf[o] = make_float4(__uint_as_float(h0), __uint_as_float(h1), __uint_as_float(l0),
+                                       __uint_as_float(l1));
+            }
+        }
         __syncthreads();
         if (KIND == 0 && kind == 2 && tid == 0) sm.down_slot = off;
         // ------------------------------------------------------ tensor-core tiles
@@ -250,7 +269,6 @@ __global__ void __launch_bounds__(kThr) mix_kernel(MixArgs a) {
                 for (int j = 0; j < NT; ++j)
 #pragma unroll
                     for (int e = 0; e < 4; ++e) ai[c][j][e] = 0.f;
-            const float *Bt = sm.B[buf];
             const int ksteps = (cnt + 7) >> 3;
             for (int kk = 0; kk < ksteps; ++kk) {
                 float av[NC][4];
@@ -274,9 +292,11 @@ __global__ void __launch_bounds__(kThr) mix_kernel(MixArgs a) {
                             av[0][idx] = b * el[rr][j];
                             av[1][idx] = b * ep[rr][j];
                         } else {
-                            const float4 s = sm.loc[on ? col : 0];
+                            // padded rows carry zero frames (leaf) and padded columns
+                            // a far dummy point with zero weight, so no masks are needed
+                            const float4 s = sm.loc[col];
                             const float dx = s.x - tl[rr][0], dy = s.y - tl[rr][1], dz = s.z - tl[rr][2];
-                            const float v = on ? val32(dx, dy, dz) : 0.f;
+                            const float v = val32(dx * dx + dy * dy + dz * dz);
                             if (KIND == 0) {
                                 av[0][idx] = v * (el[rr][0] * dx + el[rr][1] * dy + el[rr][2] * dz);
                                 av[1][idx] = v * (ep[rr][0] * dx + ep[rr][1] * dy + ep[rr][2] * dz);
@@ -293,14 +313,11 @@ __global__ void __launch_bounds__(kThr) mix_kernel(MixArgs a) {
                 for (int c = 0; c < NC; ++c)
 #pragma unroll
                     for (int e = 0; e < 4; ++e) split_tf32(av[c][e], ah[c][e], al[c][e]);
-                const int k0 = kk * 8 + t4;
 #pragma unroll
                 for (int j = 0; j < NT; ++j) {
-                    const float b0 = Bt[bofs<FT>(k0, j * 8 + g)];
-                    const float b1 = Bt[bofs<FT>(k0 + 4, j * 8 + g)];
-                    uint32_t bh0, bl0, bh1, bl1;
-                    split_tf32(b0, bh0, bl0);
-                    split_tf32(b1, bh1, bl1);
+                    const float4 bf = sm.Bf[(kk * NT + j) * 32 + lane];
+                    const uint32_t bh0 = __float_as_uint(bf.x), bh1 = __float_as_uint(bf.y);
+                    const uint32_t bl0 = __float_as_uint(bf.z), bl1 = __float_as_uint(bf.w);
 #pragma unroll
                     for (int c = 0; c < NC; ++c) {
                         mma8(ai[c][j], ah[c], bh0, bh1);
@@ -361,6 +378,8 @@ __global__ void __launch_bounds__(kThr) mix_kernel(MixArgs a) {
 }
 
 // ------------------------------------------------------------------ per-field source weights
+// kCons * area * ssh: the kernel's constant factor travels with the weights,
+// so every contraction (PP, PC, upward, CP/CC and DOWN) produces scaled results.
 __global__ void prep_mix_kernel(const double *__restrict__ area, const double *__restrict__ ssh, int64_t ld,
                                 const int32_t *__restrict__ perm, int n, int f0, int nf, int FT,
                                 float *__restrict__ wF) {
@@ -371,7 +390,7 @@ __global__ void prep_mix_kernel(const double *__restrict__ area, const double *_
     const double ar = area[pos];
     for (int f = lane; f < FT; f += 32) {
         const int ff = f0 + f;
-        wF[(size_t)pos * FT + f] = ff < nf ? (float)(ar * ssh[(size_t)ff * ld + idx]) : 0.f;
+        wF[(size_t)pos * FT + f] = ff < nf ? (float)(dev::kCons * ar * ssh[(size_t)ff * ld + idx]) : 0.f;
     }
 }
 

@@ -64,7 +64,7 @@ class GridStats(C.Structure):
         ("mode", C.c_int32), ("list_count", C.c_int64),
         ("pairs_pp", C.c_double), ("pairs_pc", C.c_double), ("pairs_cp", C.c_double), ("pairs_cc", C.c_double),
         ("macs_up", C.c_double), ("macs_down", C.c_double),
-        ("device_bytes", C.c_int64), ("setup_seconds", C.c_double),
+        ("device_bytes", C.c_int64), ("setup_seconds", C.c_double), ("mixed_bytes", C.c_int64),
     ]
 
 

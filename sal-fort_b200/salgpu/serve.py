@@ -1,0 +1,332 @@
+"""Continuous-batching request loop for SAL-gradient solves on resident grids.
+
+The reference solves one field per program run, rebuilding its tree each
+time (code.f90).  Here each registered grid keeps its tree, interaction lists,
+proxies and work plan resident in device memory; SSH fields arrive as
+requests (1..64 fields each), are batched per grid as they arrive, and each
+batch is one batched mixed-precision solve (SAL_FORM_MIXED) on the grid's own
+CUDA stream, so batches of different grids overlap on the device.
+
+Scheduling rules:
+  * a grid has at most one batch in flight (its batch buffers are its own);
+  * whenever a grid is idle and has pending requests, its oldest requests are
+    packed (whole requests, at most `max_batch` fields) into the next batch;
+  * grids are admitted to the device by an HBM budget: a grid whose resident
+    bytes (plan + batched buffers + batch staging) do not fit evicts idle
+    grids, least recently used first; a grid that alone exceeds the budget is
+    refused and its requests fail with `SalError(SAL_ENOMEM)`;
+  * requests can be cancelled until their batch is launched.
+
+Latency of a request = completion of its batch's device-to-host copy minus
+its arrival time.  Each field's result does not depend on which other fields
+share its batch (tensor-core columns never mix), which
+tests/test_serve.py checks.
+"""
+from __future__ import annotations
+
+import itertools
+import time
+from collections import OrderedDict, deque
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import FORM_MIXED, MODE_DTT, SAL_EINVAL, SAL_ENOMEM, Grid, SalError, dual_tree_traversal, tree_traverse
+
+
+@dataclass
+class Request:
+    grid: str
+    ssh: np.ndarray            # (F, N) float64, host
+    arrival: float = 0.0
+    rid: int = -1
+    status: str = "pending"    # pending | running | done | failed | cancelled
+    out_x: np.ndarray | None = None
+    out_y: np.ndarray | None = None
+    error: Exception | None = None
+    done_time: float = 0.0
+
+    @property
+    def nfields(self) -> int:
+        return self.ssh.shape[0]
+
+    @property
+    def latency(self) -> float:
+        return self.done_time - self.arrival
+
+
+@dataclass
+class GridSpec:
+    name: str
+    xs: np.ndarray
+    ys: np.ndarray
+    zs: np.ndarray
+    areas: np.ndarray
+    degree: int = 8
+    thresh: int = 200
+    theta: float = 0.7
+
+
+@dataclass
+class _Resident:
+    spec: GridSpec
+    tree: object
+    inter: np.ndarray
+    grid: Grid | None = None
+    bytes: int = 0
+    stream: object = None
+    ssh_dev: object = None
+    ox_dev: object = None
+    oy_dev: object = None
+    h_in: object = None
+    h_ox: object = None
+    h_oy: object = None
+    pending: deque = field(default_factory=deque)
+    inflight: list | None = None
+    event: object = None
+    last_used: float = 0.0
+
+
+class Server:
+    """Resident grids + per-grid continuous batching on CUDA streams."""
+
+    def __init__(self, hbm_budget_bytes: int, max_batch: int = 64, device: int = 0, clock=time.perf_counter,
+                 grid_factory=Grid):
+        try:
+            import torch
+        except ImportError:           # the CPU test double needs no torch
+            torch = None
+        self.torch = torch
+        self.budget = int(hbm_budget_bytes)
+        self.max_batch = int(max_batch)
+        self.device = device
+        self.clock = clock
+        self.grid_factory = grid_factory
+        self.grids: "OrderedDict[str, _Resident]" = OrderedDict()
+        self.used = 0
+        self._ids = itertools.count()
+        self.completed: list[Request] = []
+        self.evictions = 0
+
+    # ------------------------------------------------------------------ grids
+    def register_grid(self, spec: GridSpec) -> None:
+        """Builds the host tree and lists of a grid (tree_module.f90) once; the
+        device plan is created on admission."""
+        tree = tree_traverse(spec.xs, spec.ys, spec.zs, len(spec.xs), spec.thresh)
+        inter = dual_tree_traversal(tree, spec.theta, spec.thresh)
+        self.grids[spec.name] = _Resident(spec, tree, inter)
+
+    def _bytes_needed(self, r: _Resident, g: Grid) -> int:
+        st = g.stats()
+        n = len(r.spec.xs)
+        staging = 3 * self.max_batch * n * 8          # device ssh + two outputs
+        return int(st["device_bytes"] + st["mixed_bytes"] + staging)
+
+    def _evict(self, need: int, keep: str) -> bool:
+        for name, r in list(self.grids.items()):
+            if self.used + need <= self.budget:
+                return True
+            if name == keep or r.grid is None or r.inflight is not None:
+                continue
+            self._release(r)
+            self.evictions += 1
+        return self.used + need <= self.budget
+
+    def _release(self, r: _Resident) -> None:
+        r.grid = None
+        r.ssh_dev = r.ox_dev = r.oy_dev = None
+        self.used -= r.bytes
+        r.bytes = 0
+
+    def _admit(self, r: _Resident) -> None:
+        s = r.spec
+        g = self.grid_factory(r.tree, s.xs, s.ys, s.zs, s.areas, s.degree, MODE_DTT, r.inter, device=self.device,
+                              max_fields=self.max_batch)
+        need = self._bytes_needed(r, g)
+        if need > self.budget:
+            del g
+            raise SalError(SAL_ENOMEM, f"grid {s.name} needs {need} bytes, above the HBM budget {self.budget}")
+        if not self._evict(need, s.name):
+            del g
+            raise SalError(SAL_ENOMEM, f"no room for grid {s.name}: busy grids hold the budget")
+        r.grid = g
+        r.bytes = need
+        self.used += need
+        self._alloc_staging(r)
+
+    # ------------------------------------------------------------------ device hooks
+    # (a test double overrides these four to exercise the scheduling on the CPU)
+    def _alloc_staging(self, r: _Resident) -> None:
+        torch = self.torch
+        n = len(r.spec.xs)
+        dev = torch.device("cuda", self.device)
+        if r.stream is None:
+            r.stream = torch.cuda.Stream(device=dev)
+            r.h_in = torch.empty((self.max_batch, n), dtype=torch.float64).pin_memory()
+            r.h_ox = torch.empty((self.max_batch, n), dtype=torch.float64).pin_memory()
+            r.h_oy = torch.empty((self.max_batch, n), dtype=torch.float64).pin_memory()
+        r.ssh_dev = torch.empty((self.max_batch, n), dtype=torch.float64, device=dev)
+        r.ox_dev = torch.empty_like(r.ssh_dev)
+        r.oy_dev = torch.empty_like(r.ssh_dev)
+
+    def _launch_device(self, r: _Resident, batch: list, nf: int) -> None:
+        torch = self.torch
+        f = 0
+        for q in batch:
+            r.h_in[f:f + q.nfields].numpy()[:] = q.ssh
+            f += q.nfields
+        with torch.cuda.stream(r.stream):
+            r.ssh_dev[:nf].copy_(r.h_in[:nf], non_blocking=True)
+            r.grid.solve(r.ssh_dev[:nf], form=FORM_MIXED, out=(r.ox_dev[:nf], r.oy_dev[:nf]),
+                         stream=r.stream.cuda_stream)
+            r.h_ox[:nf].copy_(r.ox_dev[:nf], non_blocking=True)
+            r.h_oy[:nf].copy_(r.oy_dev[:nf], non_blocking=True)
+            r.event = torch.cuda.Event()
+            r.event.record(r.stream)
+
+    def _batch_done(self, r: _Resident) -> bool:
+        return r.event.query()
+
+    def _results(self, r: _Resident, f: int, nfields: int):
+        r.grid.sync()
+        return r.h_ox[f:f + nfields].numpy().copy(), r.h_oy[f:f + nfields].numpy().copy()
+
+    # ------------------------------------------------------------------ requests
+    def submit(self, req: Request) -> Request:
+        if req.grid not in self.grids:
+            raise SalError(SAL_EINVAL, f"unknown grid {req.grid}")
+        r = self.grids[req.grid]
+        n = len(r.spec.xs)
+        if req.ssh.ndim != 2 or req.ssh.shape[1] != n or not (1 <= req.nfields <= self.max_batch):
+            raise SalError(SAL_EINVAL, f"request for grid {req.grid} must be (F, {n}) with 1 <= F <= {self.max_batch}")
+        req.rid = next(self._ids)
+        if not req.arrival:
+            req.arrival = self.clock()
+        r.pending.append(req)
+        return req
+
+    def cancel(self, req: Request) -> bool:
+        r = self.grids[req.grid]
+        if req.status == "pending" and req in r.pending:
+            r.pending.remove(req)
+            req.status = "cancelled"
+            return True
+        return False
+
+    # ------------------------------------------------------------------ loop
+    def _launch(self, r: _Resident) -> None:
+        batch, nf = [], 0
+        while r.pending and nf + r.pending[0].nfields <= self.max_batch:
+            q = r.pending.popleft()
+            batch.append(q)
+            nf += q.nfields
+        if not batch:
+            return
+        if r.grid is None:
+            try:
+                self._admit(r)
+            except (SalError, MemoryError) as e:
+                for q in batch:
+                    q.status, q.error, q.done_time = "failed", e, self.clock()
+                    self.completed.append(q)
+                return
+        for q in batch:
+            q.status = "running"
+        self._launch_device(r, batch, nf)
+        r.inflight = batch
+        r.last_used = self.clock()
+        self.grids.move_to_end(r.spec.name)
+
+    def _reap(self, r: _Resident) -> None:
+        if r.inflight is None or not self._batch_done(r):
+            return
+        now = self.clock()
+        f = 0
+        for q in r.inflight:
+            try:
+                q.out_x, q.out_y = self._results(r, f, q.nfields)
+                q.status = "done"
+            except SalError as e:
+                q.status, q.error = "failed", e
+            q.done_time = now
+            f += q.nfields
+            self.completed.append(q)
+        r.inflight = None
+
+    def step(self) -> int:
+        """Reaps finished batches and launches new ones; returns the number of
+        batches in flight."""
+        for r in self.grids.values():
+            self._reap(r)
+        order = sorted((r for r in self.grids.values() if r.pending and r.inflight is None),
+                       key=lambda r: r.pending[0].arrival)
+        for r in order:
+            self._launch(r)
+        return sum(r.inflight is not None for r in self.grids.values())
+
+    def busy(self) -> bool:
+        return any(r.pending or r.inflight is not None for r in self.grids.values())
+
+    def run_until_idle(self, poll_s: float = 0.0002) -> None:
+        while self.busy():
+            if self.step() and poll_s:
+                time.sleep(poll_s)
+
+    def close(self) -> None:
+        for r in self.grids.values():
+            while r.inflight is not None:
+                self._reap(r)
+            if r.grid is not None:
+                self._release(r)
+
+
+def poisson_arrivals(rng: np.random.Generator, rate: float, duration: float) -> np.ndarray:
+    """Arrival times of a Poisson process of `rate` per second on [0, duration)."""
+    t, out = 0.0, []
+    while True:
+        t += rng.exponential(1.0 / rate)
+        if t >= duration:
+            return np.array(out)
+        out.append(t)
+
+
+def run_workload(server: Server, pools: dict, weights: dict, rate: float, duration: float, seed: int = 0,
+                 max_rhs: int = 16) -> list:
+    """Replays Poisson arrivals in real time: each request picks a grid by
+    `weights`, 1..max_rhs fields (uniform) drawn from that grid's field pool,
+    and is submitted at its arrival time while the loop keeps batching."""
+    rng = np.random.default_rng(seed)
+    times = poisson_arrivals(rng, rate, duration)
+    names = list(weights)
+    p = np.array([weights[k] for k in names], dtype=float)
+    p /= p.sum()
+    plan = []
+    for t in times:
+        name = names[rng.choice(len(names), p=p)]
+        F = int(rng.integers(1, max_rhs + 1))
+        pool = pools[name]
+        idx = rng.integers(0, pool.shape[0], size=F)
+        plan.append((t, name, idx))
+    reqs = []
+    t0 = server.clock()
+    i = 0
+    while i < len(plan) or server.busy():
+        now = server.clock() - t0
+        while i < len(plan) and plan[i][0] <= now:
+            t, name, idx = plan[i]
+            reqs.append(server.submit(Request(name, pools[name][idx], arrival=t0 + t)))
+            i += 1
+        server.step()
+    return reqs
+
+
+def summarize(reqs: list, cells: dict, wall: float) -> dict:
+    done = [q for q in reqs if q.status == "done"]
+    lat = np.array([q.latency for q in done]) * 1e3
+    evals = sum(cells[q.grid] * q.nfields for q in done)
+    single = np.array([q.latency for q in done if q.nfields == 1]) * 1e3
+    return {"requests": len(reqs), "done": len(done), "failed": sum(q.status == "failed" for q in reqs),
+            "p50_ms": float(np.percentile(lat, 50)) if len(lat) else None,
+            "p99_ms": float(np.percentile(lat, 99)) if len(lat) else None,
+            "single_field_p50_ms": float(np.percentile(single, 50)) if len(single) else None,
+            "evals_per_s": evals / wall if wall > 0 else None}
