@@ -59,6 +59,7 @@ struct GridImpl {
     int max_fields = 1;
     float *wF = nullptr, *phiF = nullptr, *mix_up_partial = nullptr, *mix_proxy_partial = nullptr;
     MixGroup *mix_leaf_groups = nullptr, *mix_proxy_groups = nullptr, *mix_up_groups = nullptr;
+    MixGroup *tc_leaf_groups = nullptr;
     Item *mix_leaf_items = nullptr, *mix_proxy_items = nullptr;
     double *tgt_nodes = nullptr;
     int64_t mix_bytes = 0;
@@ -348,6 +349,7 @@ static int ensure_mixed(GridImpl &g, int FT) {
     if (!rc) rc = dupload(g, &g.mix_proxy_groups, pl.mix_proxy_groups.data(), pl.mix_proxy_groups.size());
     if (!rc) rc = dupload(g, &g.mix_proxy_items, pl.mix_proxy_items.data(), pl.mix_proxy_items.size());
     if (!rc) rc = dupload(g, &g.mix_up_groups, pl.mix_up_groups.data(), pl.mix_up_groups.size());
+    if (!rc) rc = dupload(g, &g.tc_leaf_groups, pl.tc_leaf_groups.data(), pl.tc_leaf_groups.size());
     if (rc) return rc;
     g.FT = FT;
     g.mix_bytes = g.bytes - before;
@@ -397,11 +399,17 @@ static void solve_mixed_block(GridImpl &g, const double *ssh, int64_t ld_ssh, in
         mix::launch_finalize_mix(g.proxy_unit_beg, g.mix_proxy_partial, g.ntgt, 3 * P, FT, g.phiF, st);
     }
     if (g.timing) cudaEventRecord(g.ev[2], st);
-    a.groups = g.mix_leaf_groups;
     a.items = g.mix_leaf_items;
     a.tgt = g.pool;
     a.tgt_nodes = g.tgt_nodes;
-    mix::launch_mix(0, FT, a, (int)pl.mix_leaf_groups.size(), st);
+    if (FT == 64) {
+        // 64-field blocks: the tcgen05 leaf pass (128 targets per CTA)
+        a.groups = g.tc_leaf_groups;
+        mix::launch_tc_leaf(a, (int)pl.tc_leaf_groups.size(), g.err, st);
+    } else {
+        a.groups = g.mix_leaf_groups;
+        mix::launch_mix(0, FT, a, (int)pl.mix_leaf_groups.size(), st);
+    }
     if (g.timing) {
         cudaEventRecord(g.ev[3], st);
         cudaEventSynchronize(g.ev[3]);

@@ -34,6 +34,9 @@ void launch_prep_mix(const double *area, const double *ssh, int64_t ld, const in
 void launch_finalize_mix(const int32_t *unit_beg, const float *partial, int nslots, int rows_per_slot, int FT,
                          float *dst, cudaStream_t st);
 size_t mix_smem_bytes();
+// tcgen05 leaf pass (64-field blocks), tc_leaf.cu
+void launch_tc_leaf(const MixArgs &a, int ngroups, int *err, cudaStream_t st);
+size_t tc_smem_bytes();
 
 }  // namespace mix
 }  // namespace sal

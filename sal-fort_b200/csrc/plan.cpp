@@ -305,6 +305,7 @@ bool plan_build(const Tree &t, int d, int mode, const int32_t *list, int64_t nli
             }
         };
         pl->mix_leaf_groups.clear();
+        pl->tc_leaf_groups.clear();
         pl->mix_leaf_items.clear();
         if (dtt) {
             for (const Group &g : pl->leaf_groups) {
@@ -317,6 +318,12 @@ bool plan_build(const Tree &t, int d, int mode, const int32_t *list, int64_t nli
                     m.tgt = g.tgt + r; m.nt = std::min(kMixRows, g.nt - r); m.ib = ib; m.ie = ie; m.out = g.out;
                     m.cx = t.cx[k]; m.cy = t.cy[k]; m.cz = t.cz[k];
                     pl->mix_leaf_groups.push_back(m);
+                }
+                for (int32_t r = 0; r < g.nt; r += kTcRows) {
+                    MixGroup m{};
+                    m.tgt = g.tgt + r; m.nt = std::min(kTcRows, g.nt - r); m.ib = ib; m.ie = ie; m.out = g.out;
+                    m.cx = t.cx[k]; m.cy = t.cy[k]; m.cz = t.cz[k];
+                    pl->tc_leaf_groups.push_back(m);
                 }
             }
             pl->mix_proxy_groups.clear();

@@ -107,6 +107,7 @@ struct Plan {
     // batched form: items of at most kMixStage sources (DOWN items: rows of
     // a target slot's potentials, off = slot, cnt = rows, mask = first row)
     std::vector<MixGroup> mix_leaf_groups, mix_proxy_groups, mix_up_groups;
+    std::vector<MixGroup> tc_leaf_groups;         // leaf groups of at most kTcRows targets (tcgen05 pass)
     std::vector<Item> mix_leaf_items, mix_proxy_items;
     double pairs[4] = {0, 0, 0, 0};               // PP, PC, CP, CC evaluations per field
     double macs_up = 0, macs_down = 0;
@@ -120,6 +121,7 @@ bool plan_build(const Tree &t, int d, int mode, const int32_t *list, int64_t nli
 constexpr int kMaxStage = 256;   // sources staged per item (items are split to fit)
 constexpr int kMixStage = 64;    // sources (or DOWN rows) staged per batched item
 constexpr int kMixRows = 64;     // targets per batched CTA
+constexpr int kTcRows = 128;     // targets per tcgen05 leaf CTA (the MMA's M)
 constexpr int kMaxDegree = 14;   // a DOWN record (4(d+1)^2 + 2(d+1) doubles) fits one 8 KB stage
 
 }  // namespace sal

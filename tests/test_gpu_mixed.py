@@ -64,3 +64,24 @@ def test_mixed_batch_invariance_and_field_blocks():
     for f in range(5):
         assert rel_l2(cx[65 + f].cpu().numpy(), cy[65 + f].cpu().numpy(), ax[f].cpu().numpy(),
                       ay[f].cpu().numpy()) <= 5e-6
+
+
+def test_tcgen05_leaf_pass_matches_mma_sync_leaf_pass():
+    """Grids sized for 64-field blocks run the leaf pass on tcgen05 (tensor
+    memory accumulators); 32-field blocks run it with warp-level mma.sync.
+    Both carry the same algorithm and TF32 split, so they agree to FP32
+    rounding."""
+    torch = _torch()
+    import salgpu as S
+    g, hs = grid_and_ssh("cfg0", nfields=6, seed=9)
+    t = S.tree_traverse(g.xs, g.ys, g.zs, g.n, 100)
+    L = S.dual_tree_traversal(t, 0.7, 100)
+    g32 = S.Grid(t, g.xs, g.ys, g.zs, g.areas, 8, S.MODE_DTT, L, max_fields=32)
+    g64 = S.Grid(t, g.xs, g.ys, g.zs, g.areas, 8, S.MODE_DTT, L, max_fields=64)
+    ssh = torch.tensor(hs, device="cuda")
+    ax, ay = g32.solve(ssh, form=S.FORM_MIXED)
+    bx, by = g64.solve(ssh, form=S.FORM_MIXED)
+    torch.cuda.synchronize()
+    g64.sync()
+    for f in range(6):
+        assert rel_l2(bx[f].cpu().numpy(), by[f].cpu().numpy(), ax[f].cpu().numpy(), ay[f].cpu().numpy()) <= 2e-6
