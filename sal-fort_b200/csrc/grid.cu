@@ -60,6 +60,12 @@ struct GridImpl {
     float *wF = nullptr, *phiF = nullptr, *mix_up_partial = nullptr, *mix_proxy_partial = nullptr;
     MixGroup *mix_leaf_groups = nullptr, *mix_proxy_groups = nullptr, *mix_up_groups = nullptr;
     MixGroup *tc_leaf_groups = nullptr;
+    TcItem *tc_items = nullptr;
+    int32_t *bsrc = nullptr;
+    float *bstore = nullptr;          // split weight store of the tcgen05 leaf pass
+    float4 *sloc = nullptr;
+    double2 *selfk = nullptr;
+    int nsm = 0;
     Item *mix_leaf_items = nullptr, *mix_proxy_items = nullptr;
     double *tgt_nodes = nullptr;
     int64_t mix_bytes = 0;
@@ -349,7 +355,40 @@ static int ensure_mixed(GridImpl &g, int FT) {
     if (!rc) rc = dupload(g, &g.mix_proxy_groups, pl.mix_proxy_groups.data(), pl.mix_proxy_groups.size());
     if (!rc) rc = dupload(g, &g.mix_proxy_items, pl.mix_proxy_items.data(), pl.mix_proxy_items.size());
     if (!rc) rc = dupload(g, &g.mix_up_groups, pl.mix_up_groups.data(), pl.mix_up_groups.size());
-    if (!rc) rc = dupload(g, &g.tc_leaf_groups, pl.tc_leaf_groups.data(), pl.tc_leaf_groups.size());
+    if (!rc && FT == 64 && !pl.tc_items.empty()) {
+        // tcgen05 leaf pass: items, split weight store, per-row source
+        // coordinates and the per-point self pairs
+        rc = dupload(g, &g.tc_leaf_groups, pl.tc_leaf_groups.data(), pl.tc_leaf_groups.size());
+        if (!rc) rc = dupload(g, &g.tc_items, pl.tc_items.data(), pl.tc_items.size());
+        if (!rc) rc = dupload(g, &g.bsrc, pl.bsrc.data(), pl.bsrc.size());
+        if (!rc) rc = dalloc(g, &g.bstore, pl.bsrc.size() * 2 * (size_t)FT);
+        if (!rc) rc = dalloc(g, &g.sloc, n + (size_t)g.nsrc * P);
+        if (!rc) rc = dalloc(g, &g.selfk, n);
+        if (!rc) {
+            const size_t nr = pl.sloc_ranges.size() / 2;
+            std::vector<int2> ranges(nr);
+            std::vector<double4> centres(nr);
+            for (size_t i = 0; i < nr; ++i) {
+                ranges[i] = make_int2(pl.sloc_ranges[2 * i], pl.sloc_ranges[2 * i + 1]);
+                centres[i] = make_double4(pl.sloc_centres[3 * i], pl.sloc_centres[3 * i + 1], pl.sloc_centres[3 * i + 2], 0.0);
+            }
+            int2 *dr = nullptr;
+            double4 *dc = nullptr;
+            CK(cudaMalloc((void **)&dr, ranges.size() * sizeof(int2)));
+            cudaError_t e = cudaMalloc((void **)&dc, centres.size() * sizeof(double4));
+            if (e == cudaSuccess) e = cudaMemcpy(dr, ranges.data(), ranges.size() * sizeof(int2), cudaMemcpyHostToDevice);
+            if (e == cudaSuccess) e = cudaMemcpy(dc, centres.data(), centres.size() * sizeof(double4), cudaMemcpyHostToDevice);
+            if (e == cudaSuccess) {
+                mix::launch_source_local(g.pool, dr, dc, (int)ranges.size(), g.sloc, g.stream);
+                mix::launch_self_pair(g.pool, (int)n, g.selfk, g.stream);
+                e = cudaStreamSynchronize(g.stream);
+            }
+            cudaFree(dr);
+            if (dc) cudaFree(dc);
+            if (e != cudaSuccess) return set_error(SAL_ECUDA, std::string("batched set-up: ") + cudaGetErrorString(e));
+        }
+        if (!rc) CK(cudaDeviceGetAttribute(&g.nsm, cudaDevAttrMultiProcessorCount, g.dev));
+    }
     if (rc) return rc;
     g.FT = FT;
     g.mix_bytes = g.bytes - before;
@@ -402,10 +441,29 @@ static void solve_mixed_block(GridImpl &g, const double *ssh, int64_t ld_ssh, in
     a.items = g.mix_leaf_items;
     a.tgt = g.pool;
     a.tgt_nodes = g.tgt_nodes;
-    if (FT == 64) {
-        // 64-field blocks: the tcgen05 leaf pass (128 targets per CTA)
-        a.groups = g.tc_leaf_groups;
-        mix::launch_tc_leaf(a, (int)pl.tc_leaf_groups.size(), g.err, st);
+    if (g.bstore) {
+        // 64-field blocks: split weight store, then the tcgen05 leaf pass
+        mix::launch_split_store(g.bsrc, (int64_t)pl.bsrc.size(), g.wF, g.phiF, g.bstore, st);
+        mix::TcArgs t{};
+        t.groups = g.tc_leaf_groups;
+        t.ngroups = (int)pl.tc_leaf_groups.size();
+        t.items = g.tc_items;
+        t.sloc = g.sloc;
+        t.bstore = g.bstore;
+        t.tgt = g.pool;
+        t.xieta = g.xieta;
+        t.tgt_nodes = g.tgt_nodes;
+        t.selfk = g.selfk;
+        t.wF = g.wF;
+        t.perm = g.perm;
+        t.d = pl.d;
+        t.P = P;
+        t.out_x = ox;
+        t.out_y = oy;
+        t.ld_out = ld_out;
+        t.f0 = f0;
+        t.nf = nf;
+        mix::launch_tc_leaf(t, g.nsm, g.err, st);
     } else {
         a.groups = g.mix_leaf_groups;
         mix::launch_mix(0, FT, a, (int)pl.mix_leaf_groups.size(), st);

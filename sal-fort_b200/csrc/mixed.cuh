@@ -35,8 +35,30 @@ void launch_finalize_mix(const int32_t *unit_beg, const float *partial, int nslo
                          float *dst, cudaStream_t st);
 size_t mix_smem_bytes();
 // tcgen05 leaf pass (64-field blocks), tc_leaf.cu
-void launch_tc_leaf(const MixArgs &a, int ngroups, int *err, cudaStream_t st);
+struct TcArgs {
+    const MixGroup *groups;   // leaf groups of <= 128 targets, pool order
+    int ngroups;
+    const TcItem *items;
+    const float4 *sloc;       // per pool row: coordinates relative to the row's panel centre
+    const float *bstore;      // split weight store: 1024 floats per k-step of 8 rows
+    const double4 *tgt;       // pool (targets are its first n rows)
+    const double2 *xieta;     // per pool position
+    const double *tgt_nodes;  // 2(d+1) Chebyshev nodes per target slot
+    const double2 *selfk;     // per pool position: self pair / kernel constant
+    const float *wF;          // per pool row: 64 field weights (carry the kernel constant)
+    const int32_t *perm;      // pool position -> caller index
+    int d, P;
+    double *out_x, *out_y;    // caller's outputs (column f at + f*ld_out)
+    int64_t ld_out;
+    int f0, nf;
+};
+void launch_tc_leaf(const TcArgs &a, int nsm, int *err, cudaStream_t st);
 size_t tc_smem_bytes();
+void launch_split_store(const int32_t *bsrc, int64_t nrows, const float *wF, const float *phiF, float *bstore,
+                        cudaStream_t st);
+void launch_source_local(const double4 *pool, const int2 *ranges, const double4 *centres, int nranges, float4 *sloc,
+                         cudaStream_t st);
+void launch_self_pair(const double4 *pool, int n, double2 *selfk, cudaStream_t st);
 
 }  // namespace mix
 }  // namespace sal

@@ -319,12 +319,6 @@ bool plan_build(const Tree &t, int d, int mode, const int32_t *list, int64_t nli
                     m.cx = t.cx[k]; m.cy = t.cy[k]; m.cz = t.cz[k];
                     pl->mix_leaf_groups.push_back(m);
                 }
-                for (int32_t r = 0; r < g.nt; r += kTcRows) {
-                    MixGroup m{};
-                    m.tgt = g.tgt + r; m.nt = std::min(kTcRows, g.nt - r); m.ib = ib; m.ie = ie; m.out = g.out;
-                    m.cx = t.cx[k]; m.cy = t.cy[k]; m.cz = t.cz[k];
-                    pl->tc_leaf_groups.push_back(m);
-                }
             }
             pl->mix_proxy_groups.clear();
             pl->mix_proxy_items.clear();
@@ -348,6 +342,106 @@ bool plan_build(const Tree &t, int d, int mode, const int32_t *list, int64_t nli
                     m.ie = pl->up_units[u].end; m.out = (int32_t)u; m.row0 = r;
                     pl->mix_up_groups.push_back(m);
                 }
+        }
+    }
+    // ---------------------------------------------------------------- tcgen05 leaf pass
+    // The split weight store holds every source row of the leaf pass once, as
+    // TF32 hi/lo tiles per k-step of 8 rows: each leaf's points, then each
+    // source slot's P proxies, then each target slot's 3P potential rows, every
+    // range padded with zero rows to a multiple of 8 so that each item starts
+    // on a k-step boundary and its padding columns meet zero weights.
+    pl->tc_items.clear();
+    pl->bsrc.clear();
+    pl->sloc_ranges.clear();
+    pl->sloc_centres.clear();
+    if (dtt) {
+        auto add_range = [&](int64_t b, int64_t e, int k) {
+            pl->sloc_ranges.push_back((int32_t)b);
+            pl->sloc_ranges.push_back((int32_t)e);
+            pl->sloc_centres.push_back(t.cx[k]);
+            pl->sloc_centres.push_back(t.cy[k]);
+            pl->sloc_centres.push_back(t.cz[k]);
+        };
+        for (int k : leaves) add_range(t.p[k].begin, t.p[k].end, k);
+        for (int32_t s = 0; s < nsrc; ++s) add_range(n + (int64_t)s * P, n + (int64_t)(s + 1) * P, pl->src_slot_panel[s]);
+        auto up8 = [](int64_t x) { return (x + 7) & ~int64_t(7); };
+        std::vector<int64_t> leaf_b(leaves.size());
+        int64_t nb = 0;
+        for (size_t i = 0; i < leaves.size(); ++i) { leaf_b[i] = nb; nb += up8(t.p[leaves[i]].count()); }
+        const int64_t src_b0 = nb, P8 = up8(P), P38 = up8(3 * P);
+        nb += (int64_t)nsrc * P8;
+        const int64_t phi_b0 = nb;
+        nb += (int64_t)ntgt * P38;
+        if (nb / 8 > INT32_MAX / 2) { *err = "grid too large for the split weight store"; return false; }
+        pl->bsrc.assign((size_t)nb, -1);
+        for (size_t i = 0; i < leaves.size(); ++i) {
+            const Panel &q = t.p[leaves[i]];
+            for (int64_t p = q.begin; p < q.end; ++p) pl->bsrc[leaf_b[i] + (p - q.begin)] = (int32_t)p;
+        }
+        for (int32_t s = 0; s < nsrc; ++s)
+            for (int r = 0; r < P; ++r) pl->bsrc[src_b0 + s * P8 + r] = (int32_t)(n + (int64_t)s * P + r);
+        for (int32_t s = 0; s < ntgt; ++s)
+            for (int r = 0; r < 3 * P; ++r) pl->bsrc[phi_b0 + s * P38 + r] = (int32_t)(-2 - ((int64_t)s * 3 * P + r));
+        std::vector<int32_t> gord(pl->leaf_groups.size());
+        std::iota(gord.begin(), gord.end(), 0);
+        std::sort(gord.begin(), gord.end(), [&](int a, int b) { return pl->leaf_groups[a].tgt < pl->leaf_groups[b].tgt; });
+        for (int32_t gi : gord) {
+            const Group &g = pl->leaf_groups[gi];
+            const int kt = leaves[g.out];
+            const int32_t ib = (int32_t)pl->tc_items.size();
+            auto push = [&](int kind, int64_t off, int64_t total, int64_t base, int ks) {
+                TcItem r{};
+                r.kind = kind;
+                if (ks >= 0) {
+                    r.dx = (float)(t.cx[ks] - t.cx[kt]);
+                    r.dy = (float)(t.cy[ks] - t.cy[kt]);
+                    r.dz = (float)(t.cz[ks] - t.cz[kt]);
+                }
+                for (int64_t b = 0; b < total; b += kTcChunk) {
+                    r.cnt = (int32_t)std::min<int64_t>(kTcChunk, total - b);
+                    r.kb = (int32_t)((base + b) / 8);
+                    r.off = (int32_t)(kind == 2 ? off : off + b);
+                    r.row0 = kind == 2 ? (int32_t)b : 0;
+                    pl->tc_items.push_back(r);
+                }
+            };
+            for (int32_t i = g.ib; i < g.ie; ++i) {
+                const Item &it = pl->leaf_items[i];
+                if (it.kind == 0) {
+                    // a PP source panel's range, re-joined across the staging
+                    // splits and cut at leaf boundaries
+                    int64_t b = it.off, e = (int64_t)it.off + it.cnt;
+                    while (i + 1 < g.ie && pl->leaf_items[i + 1].kind == 0 && pl->leaf_items[i + 1].off == e)
+                        e += pl->leaf_items[++i].cnt;
+                    while (b < e) {
+                        const int32_t l = leaf_of_pos[b];
+                        const Panel &q = t.p[leaves[l]];
+                        const int64_t le = std::min<int64_t>(e, q.end);
+                        if ((b - q.begin) % 8 != 0) { *err = "internal: PP range starts inside a leaf"; return false; }
+                        push(0, b, le - b, leaf_b[l] + (b - q.begin), leaves[l]);
+                        b = le;
+                    }
+                } else if (it.kind == 1) {
+                    const int64_t s = ((int64_t)it.off - n) / P;
+                    push(1, it.off, it.cnt, src_b0 + s * P8, pl->src_slot_panel[s]);
+                } else {
+                    push(2, it.off, 3 * P, phi_b0 + (int64_t)it.off * P38, -1);
+                }
+            }
+            const int32_t ie = (int32_t)pl->tc_items.size();
+            // accumulator chains: end one after the item that brings it to
+            // kTcChainKSteps k-steps, and always after the group's last item
+            for (int32_t i = ib, chain = 0; i < ie; ++i) {
+                TcItem &r = pl->tc_items[i];
+                chain += (r.cnt + 7) / 8;
+                if (chain >= kTcChainKSteps || i == ie - 1) { r.kind |= kTcFlush; chain = 0; }
+            }
+            for (int32_t r = 0; r < g.nt; r += kTcRows) {
+                MixGroup m{};
+                m.tgt = g.tgt + r; m.nt = std::min(kTcRows, g.nt - r); m.ib = ib; m.ie = ie; m.out = g.out;
+                m.cx = t.cx[kt]; m.cy = t.cy[kt]; m.cz = t.cz[kt];
+                pl->tc_leaf_groups.push_back(m);
+            }
         }
     }
     // ---------------------------------------------------------------- point data in pool order

@@ -82,6 +82,21 @@ struct MixGroup {
     double cx, cy, cz, pad2;
 };
 
+// Item of the tcgen05 leaf pass.  kind & 3 = 0 / 1: sources are pool rows
+// [off, off + cnt); kind & 3 = 2: rows [row0, row0 + cnt) of target slot
+// off's Cartesian potentials.  kind & kTcFlush: the tensor-core accumulator
+// chain ends after this item (its sum is folded into the running sum with
+// round-to-nearest adds).  kb: first k-step (8 rows) of the item in the split
+// weight store.  (dx, dy, dz): centre of the source panel minus centre of the
+// target leaf (kinds 0, 1), so that source coordinates stored relative to
+// their own panel centre become coordinates relative to the target leaf.
+constexpr int32_t kTcFlush = 4;
+struct TcItem {
+    int32_t off, cnt, kb, kind;
+    float dx, dy, dz;
+    int32_t row0;
+};
+
 struct Plan {
     int32_t n = 0, d = 0, P = 0, mode = 0, npanels = 0, nleaves = 0;
     // point data in pool order (leaf-contiguous DFS)
@@ -107,7 +122,17 @@ struct Plan {
     // batched form: items of at most kMixStage sources (DOWN items: rows of
     // a target slot's potentials, off = slot, cnt = rows, mask = first row)
     std::vector<MixGroup> mix_leaf_groups, mix_proxy_groups, mix_up_groups;
-    std::vector<MixGroup> tc_leaf_groups;         // leaf groups of at most kTcRows targets (tcgen05 pass)
+    // tcgen05 leaf pass: groups of at most kTcRows targets in pool order, their
+    // items and the row map of the split weight store (per store row: wF row
+    // if >= 0, phiF row -2-v if <= -2, zero row if -1; every leaf, source
+    // slot and target slot starts on a multiple of 8 rows).
+    std::vector<MixGroup> tc_leaf_groups;
+    std::vector<TcItem> tc_items;
+    std::vector<int32_t> bsrc;
+    // pool row ranges (begin, end) of every leaf and every source slot's
+    // proxies, with the centre (x, y, z) of the range's panel
+    std::vector<int32_t> sloc_ranges;
+    std::vector<double> sloc_centres;
     std::vector<Item> mix_leaf_items, mix_proxy_items;
     double pairs[4] = {0, 0, 0, 0};               // PP, PC, CP, CC evaluations per field
     double macs_up = 0, macs_down = 0;
@@ -121,7 +146,9 @@ bool plan_build(const Tree &t, int d, int mode, const int32_t *list, int64_t nli
 constexpr int kMaxStage = 256;   // sources staged per item (items are split to fit)
 constexpr int kMixStage = 64;    // sources (or DOWN rows) staged per batched item
 constexpr int kMixRows = 64;     // targets per batched CTA
-constexpr int kTcRows = 128;     // targets per tcgen05 leaf CTA (the MMA's M)
+constexpr int kTcRows = 128;     // targets per tcgen05 leaf group (the MMA's M)
+constexpr int kTcChunk = 64;     // sources (or DOWN rows) per tcgen05 item
+constexpr int kTcChainKSteps = 32;  // k-steps (8 sources) an accumulator chain reaches before it is folded
 constexpr int kMaxDegree = 14;   // a DOWN record (4(d+1)^2 + 2(d+1) doubles) fits one 8 KB stage
 
 }  // namespace sal

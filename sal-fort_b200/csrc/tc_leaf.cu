@@ -1,27 +1,36 @@
 // Leaf pass of the batched form on the 5th-generation tensor cores (tcgen05).
 //
-// One CTA = one leaf group of up to 128 targets (the MMA's M) x 64 fields.
-// Warps 0-7 produce: thread t < 256 owns target row r = t % 128 and half
-// h = t / 128 of every 8-column k-step.  Warp 8 only issues the MMAs, so no
-// producer warp diverges around the issue (a lane blocked in an mbarrier wait
-// would otherwise hold up the lane that must issue).  Per item (<= 64
-// sources, or <= 64 Cartesian rows of a DOWN interpolation) the CTA
-//   1. waits for the item's per-field rows (cp.async), folds the previous
-//      item's accumulator into the running sum (both in tensor memory), and
-//      rewrites the rows as TF32 hi / lo B tiles in the canonical no-swizzle
-//      K-major layout;
-//   2. for each k-step, every producer thread forms its 4 kernel-tile entries
-//      in FP32 (east and north components, hi and lo parts) into one of two
-//      shared A slots; the MMA warp issues the six tcgen05.mma of the k-step
-//      (hi*hi + hi*lo + lo*hi for each component) into the item accumulator
-//      and commits them to the slot's "empty" barrier.
-// The item accumulator starts from zero at every item and is added to the
-// running sum with round-to-nearest FP32 adds: the tensor cores accumulate
-// with truncation, so chaining all k-steps of a target in one accumulator
-// biases the result toward zero.
-// Tensor memory (256 columns): item accumulator [east 64 | north 64] at
-// columns 0..127, running sum at 128..255.  Shared memory ~102 KB, so at most
-// two CTAs share an SM and their 2 x 256 columns fit the 512 the SM has.
+// Persistent kernel, one CTA per SM, walking leaf groups of up to 128 targets
+// in pool order with a stride of the grid size.  A group's work is a list of
+// items (<= 64 sources, or <= 64 Cartesian rows of a DOWN interpolation), cut
+// into stages of 16 K columns (two k-steps of 8).  The contraction is
+//     D[field part, target component] += W[field part, k] * T[k, target component]
+// with M = 128 weight rows (64 fields, TF32 hi and lo parts, ordered so that
+// field f's hi row 32(f/16) + f%16 and lo row +16 share a warp) and N = 256
+// kernel-tile columns (east of the 128 targets, then north).  One tcgen05.mma
+// costs the same whatever its N, so N = 256 keeps the tensor cores at full
+// width: per k-step two MMAs, W * T_hi and W * T_lo, give all four hi/lo
+// cross products.
+// Warp roles:
+//   warps 0-7   producers.  Thread t forms target row t % 128 of k-step t / 128
+//               of every stage: 8 kernel-tile entries per component in FP32,
+//               split into TF32 hi + lo, stored to shared memory in the
+//               canonical K-major layout (the MMA's B operand).  The self
+//               pair enters as the tile's diagonal entry: the reference
+//               kernel's FP64 value at distance zero (rounding noise).
+//   warp 8      issues the MMAs.
+//   warp 9      loads, per stage, the weight tiles (pre-split TF32 hi / lo,
+//               written once per solve by split_store_kernel) and the sources'
+//               FP32 coordinates with bulk copies into a 4-deep ring.
+//   warps 10-13 fold finished accumulator chains into the running sums and
+//               write the outputs (warp w: tensor memory lanes 32(w%4)..+31).
+// The tensor cores accumulate with truncation, so one chain over all of a
+// target's sources would bias the result toward zero: a chain ends after about
+// 32 k-steps (plan flag kTcFlush); its hi and lo rows are added and folded into
+// the group's running sums (shared memory, FP32, round to nearest).  Two
+// accumulators in tensor memory (columns 0-255 and 256-511) alternate between
+// chains, so the tensor cores go on with the next chain while the fold warps
+// fold the last one.
 #include <cuda_runtime.h>
 
 #include "kernels.cuh"
@@ -34,60 +43,61 @@ using dev::smem_u32;
 
 namespace {
 
-constexpr int kThreads = 288;    // 8 producer warps + 1 MMA warp
-constexpr int kProducers = 256;
-constexpr int kRows = kTcRows;   // 128
-constexpr int kF = 64;           // fields per CTA (the MMA's N per component)
-constexpr int kK = kMixStage;    // 64 K rows per item
-constexpr int kTmemCols = 256;
+constexpr int kProdWarps = 8;
+constexpr int kProducers = kProdWarps * 32;      // one per (target row, k-step of a stage)
+constexpr int kMmaWarp = kProdWarps;
+constexpr int kLoadWarp = kProdWarps + 1;
+constexpr int kFoldWarps = 4;                     // one per tensor memory lane quarter
+constexpr int kThreads = (kProdWarps + 2 + kFoldWarps) * 32;   // 448
+constexpr int kF = 64;                            // fields
+constexpr int kStageK = 16;                       // K columns per stage (two k-steps of 8)
+constexpr int kKStages = 3;                       // kernel-tile ring
+constexpr int kWStages = 4;                       // weight / coordinate ring
+constexpr int kTileFloats = 2048;                 // kernel tile of one k-step: 256 rows x 8, one of hi / lo
+constexpr int kWStepFloats = 1024;                // weight tile of one k-step: 128 rows x 8
+constexpr int kTmemCols = 512;
+constexpr int kKmap = 3 * (kMaxDegree + 1) * (kMaxDegree + 1) + 64;
+constexpr uint32_t kWaitPolls = 1u << 22;
 constexpr float kC1F = (float)dev::kC1;
 constexpr float kTwoC2F = (float)(2.0 * dev::kC2);
 
-// instruction descriptor: D F32, A/B TF32, both K-major, N = 64, M = 128
-constexpr uint32_t kIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(kF >> 3) << 17) |
-                            ((uint32_t)(kRows >> 4) << 24);
+static_assert(kTcChunk % kStageK == 0, "items are whole stages");
+
+// instruction descriptor: D F32, A/B TF32, both K-major, N = 256, M = 128
+constexpr uint32_t kIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(256 >> 3) << 17) |
+                            ((uint32_t)(128 >> 4) << 24);
 
 struct TcSmem {
-    float4 A[2][4][kRows * 2];          // 2 slots x {east hi, east lo, north hi, north lo} x 128 rows x 8 tf32
-    float4 B[kK / 8][2][kF * 2];        // per k-step: {hi, lo} x 64 fields x 8 tf32 (canonical K-major)
-    float Bp[kK * kF];                  // rows as copied (cp.async), XOR-swizzled 16-byte chunks
-    double4 raw[kK];
-    float4 loc[kK];
-    float fx[kRows][kMaxDegree + 1];    // BLI bases of the row targets in the current DOWN panel
-    float fe[kRows][kMaxDegree + 1];
-    int kmap[3 * (kMaxDegree + 1) * (kMaxDegree + 1) + 8];
-    uint64_t full[2], empty[2], item_done;
+    float Kt[kKStages][2][2][kTileFloats];       // per stage: k-step x {hi, lo} x 256 rows x 8
+    float Wt[kWStages][2 * kWStepFloats];        // per stage: 2 k-steps x 128 weight rows x 8
+    float4 loc[kWStages][kStageK];               // per stage: source coordinates of its 16 columns
+    float run[2 * kTcRows][kF];                  // running sums: [component x target][field, 16-blocks swapped on odd targets]
+    float fx[kTcRows][kMaxDegree + 1];           // per target row: BLI bases in the current DOWN slot
+    float fe[kTcRows][kMaxDegree + 1];
+    int kmap[kKmap];
+    uint64_t kfull[kKStages], kempty[kKStages], wfull[kWStages], wempty[kWStages], accfull[2], accfree[2], fin;
     uint32_t tmem_base;
-    int down_slot;
     int abort;
 };
 
 __device__ __forceinline__ float val32(float mp) {
+    // mp = 0 only for a source on the target itself (or a repeated point),
+    // where the projected displacement is exactly 0: the clamp keeps the
+    // value finite so that the entry is 0.
+    mp = fmaxf(mp, 1e-20f);
     float r, u;
     asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(mp));
     const float q = mp * r;
     asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(u) : "f"(2.f + q));
     const float inner = fmaf(kC1F, r, fmaf(kTwoC2F, u, -kTwoC2F));
-    const float v = inner * r * r;
-    return mp > 0.f ? v : 0.f;
+    return inner * r * r;
 }
 
-__device__ __forceinline__ uint32_t to_tf32(float x) {
+__device__ __forceinline__ float tf32_hi(float x) {
     uint32_t r;
     asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
-    return r;
+    return __uint_as_float(r);
 }
-__device__ __forceinline__ void split(float x, float &hi, float &lo) {
-    const uint32_t h = to_tf32(x);
-    hi = __uint_as_float(h);
-    lo = __uint_as_float(to_tf32(x - hi));
-}
-
-__device__ __forceinline__ void cp16(void *dst, const void *src) {
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
-}
-__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void cp_wait0() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
 
 __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
@@ -96,11 +106,21 @@ __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
 // the CTA-wide abort flag (later waits then return at once).
 __device__ __forceinline__ void wait_bounded(uint64_t *bar, uint32_t parity, volatile int *abort, int *err) {
     if (*abort) return;
-    for (uint32_t it = 0; it < (1u << 24); ++it)
+    for (uint32_t it = 0; it < kWaitPolls; ++it)
         if (dev::mbar_try_wait(bar, parity)) return;
     *abort = 1;
     atomicExch(err, dev::kErrTimeout);
 }
+// Bounded wait that ignores the abort flag (drains copies and MMAs in flight
+// before the CTA exits).
+__device__ __forceinline__ void wait_drain(uint64_t *bar, uint32_t parity, int *err) {
+    for (uint32_t it = 0; it < kWaitPolls; ++it)
+        if (dev::mbar_try_wait(bar, parity)) return;
+    atomicExch(err, dev::kErrTimeout);
+}
+
+// Named barrier 1 over the producer warps.
+__device__ __forceinline__ void producers_sync() { asm volatile("bar.sync 1, %0;" ::"r"(kProducers) : "memory"); }
 
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
@@ -114,7 +134,8 @@ __device__ __forceinline__ uint64_t smem_desc(const void *p) {
            (1ull << 46);
 }
 
-__device__ __forceinline__ void mma_tf32(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t accumulate) {
+// D[tmem] (+)= A[smem] * B[smem]
+__device__ __forceinline__ void mma_ss(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t accumulate) {
     asm volatile(
         "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
         "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d_tmem),
@@ -137,35 +158,77 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
 #pragma unroll
     for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
-__device__ __forceinline__ void tmem_st16(uint32_t taddr, const float (&v)[16]) {
-    asm volatile(
-        "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
-        "%14, %15, %16};" ::"r"(taddr),
-        "r"(__float_as_uint(v[0])), "r"(__float_as_uint(v[1])), "r"(__float_as_uint(v[2])),
-        "r"(__float_as_uint(v[3])), "r"(__float_as_uint(v[4])), "r"(__float_as_uint(v[5])),
-        "r"(__float_as_uint(v[6])), "r"(__float_as_uint(v[7])), "r"(__float_as_uint(v[8])),
-        "r"(__float_as_uint(v[9])), "r"(__float_as_uint(v[10])), "r"(__float_as_uint(v[11])),
-        "r"(__float_as_uint(v[12])), "r"(__float_as_uint(v[13])), "r"(__float_as_uint(v[14])),
-        "r"(__float_as_uint(v[15]))
-        : "memory");
-}
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
-__device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
 
-// Byte offset of element (row, k) of a canonical K-major tile (k < 8).
-__device__ __forceinline__ int canon(int row, int k) {
+// BLI basis (FP64, stored as FP32) of one coordinate of a target over one
+// axis's Chebyshev nodes.  Out of line: its local array stays out of the
+// stage loop's registers.
+__device__ __noinline__ void down_basis(double x, const double *nodes, int n, float *out) {
+    double f[kMaxDegree + 1];
+    dev::bli_basis(x, nodes, n, f);
+    for (int i = 0; i < n; ++i) out[i] = (float)f[i];
+}
+
+// Byte offset of element (row, k) of a canonical K-major tile without
+// swizzle (8-row x 16-byte core matrices, K halves 128 B apart, 8-row groups
+// 256 B apart), k < 8.
+__host__ __device__ constexpr int canon(int row, int k) {
     return (row >> 3) * 256 + (k >> 2) * 128 + (row & 7) * 16 + (k & 3) * 4;
 }
+// Weight-tile row of field f's hi (part 0) or lo (part 1) TF32 part: the two
+// rows of a field sit in one 32-lane quarter of the accumulator, 16 apart.
+__host__ __device__ constexpr int wrow(int f, int part) { return 32 * (f >> 4) + 16 * part + (f & 15); }
 
 }  // namespace
 
-__global__ void __launch_bounds__(kThreads, 2) tc_leaf_kernel(MixArgs a, int *err) {
+// Folds a finished accumulator chain (warp-collective; this warp's lane
+// quarter q: fields 16q..16q+15 of both components for the group's 128
+// target slots).  Lanes 0-15 hold the chain's hi rows, lanes 16-31 the same
+// fields' lo rows; per column pair, lanes 0-15 take the even column and lanes
+// 16-31 the odd one, so hi + lo of a field meet in one lane.  Mid-group:
+// running sum (+)= chain (the group's first chain stores).  At the group's
+// end: running sum + chain to the caller's outputs for its nt targets.
+__device__ __noinline__ void fold_chain(uint32_t td, float *run, int q, int lane, bool end, bool first, int tgt,
+                                        int nt, const int32_t *__restrict__ perm, double *out_x, double *out_y,
+                                        int64_t ld_out, int f0, int nf, bool skip) {
+    const int f = 16 * q + (lane & 15), odd = lane >> 4;
+    int idx[4] = {0, 0, 0, 0};   // caller index of target slot 32k + lane
+    if (end)
+#pragma unroll
+        for (int k = 0; k < 4; ++k) idx[k] = 32 * k + lane < nt ? perm[tgt + 32 * k + lane] : 0;
+#pragma unroll 1
+    for (int cc = 0; cc < 256; cc += 16) {
+        const int ch = cc >> 7, c0 = cc & 127;
+        if (end && c0 >= nt) continue;
+        float x[16];
+        tmem_ld16(td + cc, x);
+        tmem_wait_ld();
+        const int ik = c0 >> 5;
+        const int idk = ik == 0 ? idx[0] : ik == 1 ? idx[1] : ik == 2 ? idx[2] : idx[3];
+        double *out = ch == 0 ? out_x : out_y;
+#pragma unroll
+        for (int m = 0; m < 8; ++m) {
+            const float lo_even = __shfl_down_sync(0xffffffffu, x[2 * m], 16);
+            const float hi_odd = __shfl_up_sync(0xffffffffu, x[2 * m + 1], 16);
+            const float v = odd ? x[2 * m + 1] + hi_odd : x[2 * m] + lo_even;
+            const int t = c0 + 2 * m + odd;                 // target slot
+            // odd target slots store their fields with the 16-blocks swapped,
+            // so the two half-warps hit different banks
+            float *rp = run + (size_t)(128 * ch + t) * kF + (f ^ (odd << 4));
+            const float sum = first ? v : *rp + v;
+            const int ti = __shfl_sync(0xffffffffu, idk, t & 31);
+            if (!end)
+                *rp = sum;
+            else if (t < nt && f0 + f < nf && !skip)
+                out[(size_t)(f0 + f) * ld_out + ti] = (double)sum;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(TcArgs a, int *err) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     TcSmem &sm = *reinterpret_cast<TcSmem *>(smem_raw);
-    const MixGroup G = a.groups[blockIdx.x];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const bool producer = tid < kProducers;
-    const int row = tid & (kRows - 1), half = (tid >> 7) & 1;
     const int n = a.d + 1, P = a.P;
     volatile int *abort = &sm.abort;
 
@@ -178,241 +241,271 @@ __global__ void __launch_bounds__(kThreads, 2) tc_leaf_kernel(MixArgs a, int *er
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
     if (tid == 0) {
-        dev::mbar_init(&sm.full[0], kProducers);
-        dev::mbar_init(&sm.full[1], kProducers);
-        dev::mbar_init(&sm.empty[0], 1);
-        dev::mbar_init(&sm.empty[1], 1);
-        dev::mbar_init(&sm.item_done, 1);
+        for (int j = 0; j < kKStages; ++j) {
+            dev::mbar_init(&sm.kfull[j], kProdWarps);
+            dev::mbar_init(&sm.kempty[j], 1);
+        }
+        for (int j = 0; j < kWStages; ++j) {
+            dev::mbar_init(&sm.wfull[j], 1);
+            dev::mbar_init(&sm.wempty[j], 1);
+        }
+        for (int j = 0; j < 2; ++j) {
+            dev::mbar_init(&sm.accfull[j], 1);
+            dev::mbar_init(&sm.accfree[j], kFoldWarps);
+        }
+        dev::mbar_init(&sm.fin, 1);
         dev::fence_mbar_init();
-        sm.down_slot = -1;
         sm.abort = 0;
     }
-    for (int k = tid; k < 3 * P + 8; k += kThreads) {
+    for (int k = tid; k < kKmap; k += kThreads) {
         const int kk = k < 3 * P ? k : 0;
         const int p = kk / 3;
         sm.kmap[k] = (p % n) | ((p / n) << 8) | ((kk % 3) << 16);
     }
-    // the row's target: coordinates relative to the leaf centre and its
-    // east / north unit vectors scaled by nothing (the reference's 1/sqrt(1-z^2)
-    // is part of the unit vectors' normalisation)
-    const bool rvalid = producer && row < G.nt;
-    float tl0 = 0.f, tl1 = 0.f, tl2 = 0.f, el0 = 0.f, el1 = 0.f, ep0 = 0.f, ep1 = 0.f, ep2 = 0.f;
-    if (rvalid) {
-        const double4 c = a.tgt[G.tgt + row];
-        tl0 = (float)(c.x - G.cx);
-        tl1 = (float)(c.y - G.cy);
-        tl2 = (float)(c.z - G.cz);
-        if ((fabs(c.z - 1.0) > 1e-15) && (fabs(c.z + 1.0) > 1e-15)) {
-            const double omz = 1.0 - c.z * c.z, inv = 1.0 / sqrt(omz);
-            el0 = (float)(-c.y * inv);
-            el1 = (float)(c.x * inv);
-            ep0 = (float)(-c.z * c.x * inv);
-            ep1 = (float)(-c.z * c.y * inv);
-            ep2 = (float)(omz * inv);
-        }
-    }
+    // columns past an item's sources read these until a copy overwrites them
+    for (int k = tid; k < kWStages * kStageK; k += kThreads)
+        sm.loc[k / kStageK][k % kStageK] = make_float4(4.f, 4.f, 4.f, 0.f);
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = sm.tmem_base;
-    const uint32_t lane_base = (uint32_t)(32 * (warp & 3)) << 16;   // this warp's TMEM lane quarter
-    const uint32_t run_col = 128 + 64 * half;                      // running sum: east (half 0) / north (half 1)
-    const uint32_t item_col = 64 * half;
-    if (producer) {
-        float z[16];
-#pragma unroll
-        for (int i = 0; i < 16; ++i) z[i] = 0.f;
-#pragma unroll
-        for (int c = 0; c < 4; ++c) tmem_st16(tmem + lane_base + run_col + 16 * c, z);
-        tmem_wait_st();
-    }
+    uint32_t st = 0;   // stages this CTA has gone through
 
-    const int ni = G.ie - G.ib;
-    auto prefetch = [&](int k) {
-        const Item it = a.items[G.ib + k];
-        const float *src = it.kind == 2 ? a.phiF + ((size_t)it.off * 3 * P + it.mask) * kF
-                                        : a.wF + (size_t)it.off * kF;
-        if (it.kind != 2)
-            for (int i = tid; i < it.cnt * 2; i += kThreads)
-                cp16(reinterpret_cast<char *>(&sm.raw[i >> 1]) + 16 * (i & 1),
-                     reinterpret_cast<const char *>(a.pool + it.off + (i >> 1)) + 16 * (i & 1));
-        constexpr int CH = kF / 4;
-        for (int i = tid; i < it.cnt * CH; i += kThreads) {
-            const int r = i / CH, c = i % CH;
-            cp16(&sm.Bp[r * kF + ((c ^ ((r & 3) << 1)) << 2)], src + (size_t)r * kF + c * 4);
-        }
-    };
-    auto flush = [&]() {
-        // running sum += item accumulator (this warp's 32 lanes x 64 columns)
-#pragma unroll
-        for (int c = 0; c < 4; ++c) {
-            float x[16], y[16];
-            tmem_ld16(tmem + lane_base + item_col + 16 * c, x);
-            tmem_ld16(tmem + lane_base + run_col + 16 * c, y);
-            tmem_wait_ld();
-#pragma unroll
-            for (int i = 0; i < 16; ++i) y[i] += x[i];
-            tmem_st16(tmem + lane_base + run_col + 16 * c, y);
-        }
-        tmem_wait_st();
-    };
+    if (warp < kProdWarps) {
+        // ============================================================ producers
+        const int row = tid & (kTcRows - 1), ks = tid >> 7;      // generation: target row, k-step of the stage
+        // canonical offsets (floats) of this thread's east / north rows in a kernel tile
+        const int oe = canon(row, 0) >> 2, on = canon(kTcRows + row, 0) >> 2;
+        // wait for a free kernel-tile slot
+        auto wait_slot = [&](uint32_t s) {
+            if (s >= (uint32_t)kKStages)
+                wait_bounded(&sm.kempty[s % kKStages], ((s / kKStages) - 1) & 1, abort, err);
+        };
 
-    if (ni > 0) prefetch(0);
-    cp_commit();
-    uint32_t gk = 0;   // k-steps issued so far by this CTA
-    for (int k = 0; k < ni; ++k) {
-        cp_wait0();
-        __syncthreads();
-        const Item it = a.items[G.ib + k];
-        const int cnt = it.cnt, ks = (cnt + 7) >> 3, kend = ks * 8;
-        if (k > 0 && producer) {
-            wait_bounded(&sm.item_done, (uint32_t)((k - 1) & 1), abort, err);
-            tc_fence_after();
-            flush();
-        }
-        // ------------------------------------------------ item preparation
-        if (it.kind != 2) {
-            if (tid < cnt) {
-                const double4 s = sm.raw[tid];
-                sm.loc[tid] = make_float4((float)(s.x - G.cx), (float)(s.y - G.cy), (float)(s.z - G.cz), 0.f);
-            } else if (tid < kend) {
-                sm.loc[tid] = make_float4(4.f, 4.f, 4.f, 0.f);   // padding column: finite entries, zero weights
-            }
-        } else if (sm.down_slot != it.off && tid < kRows) {   // producers of half 0
-            float *fxr = sm.fx[tid], *fer = sm.fe[tid];
-            if (tid < G.nt) {
-                const double2 e = a.xieta[G.tgt + tid];
-                const double *nodes = a.tgt_nodes + (size_t)it.off * 2 * n;
-                double f[kMaxDegree + 1];
-                dev::bli_basis(e.x, nodes, n, f);
-                for (int i = 0; i < n; ++i) fxr[i] = (float)f[i];
-                dev::bli_basis(e.y, nodes + n, n, f);
-                for (int i = 0; i < n; ++i) fer[i] = (float)f[i];
-            } else {
-                for (int i = 0; i < n; ++i) fxr[i] = fer[i] = 0.f;
-            }
-        }
-        // B rows -> TF32 hi / lo tiles, canonical K-major (rows = fields, K = sources)
-        for (int e = tid; e < kend * kF; e += kThreads) {
-            const int f = e & (kF - 1), kr = e >> 6;
-            const float v = kr < cnt ? sm.Bp[kr * kF + ((((f >> 2) ^ ((kr & 3) << 1))) << 2) + (f & 3)] : 0.f;
-            float hi, lo;
-            split(v, hi, lo);
-            const int off = canon(f, kr & 7);
-            reinterpret_cast<float *>(sm.B[kr >> 3][0])[off >> 2] = hi;
-            reinterpret_cast<float *>(sm.B[kr >> 3][1])[off >> 2] = lo;
-        }
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        tc_fence_before();
-        __syncthreads();
-        tc_fence_after();
-        if (tid == 0 && it.kind == 2) sm.down_slot = it.off;
-        if (k + 1 < ni) prefetch(k + 1);
-        cp_commit();
-        // ------------------------------------------------ k-steps
-        for (int s = 0; s < ks; ++s, ++gk) {
-            const uint32_t slot = gk & 1, use = gk >> 1;
-            if (!producer) {
-                // the MMA warp: wait for the slot, issue the k-step's six MMAs
-                wait_bounded(&sm.full[slot], use & 1, abort, err);
-                tc_fence_after();
-                if (lane == 0) {
-                    if (!*abort) {
-                        const uint64_t bh = smem_desc(sm.B[s][0]), bl = smem_desc(sm.B[s][1]);
-#pragma unroll
-                        for (int comp = 0; comp < 2; ++comp) {
-                            const uint32_t d = tmem + 64 * comp;
-                            const uint64_t ah = smem_desc(sm.A[slot][2 * comp]);
-                            const uint64_t al = smem_desc(sm.A[slot][2 * comp + 1]);
-                            mma_tf32(d, ah, bh, s > 0 ? 1u : 0u);
-                            mma_tf32(d, ah, bl, 1u);
-                            mma_tf32(d, al, bh, 1u);
-                        }
-                    }
-                    mma_commit(&sm.empty[slot]);
-                    if (s == ks - 1) mma_commit(&sm.item_done);
+        for (int gi = blockIdx.x; gi < a.ngroups; gi += gridDim.x) {
+            const MixGroup G = a.groups[gi];
+            const int ni = G.ie - G.ib;
+            const bool active = (row & ~31) < G.nt, rvalid = row < G.nt;
+            // the row's target relative to the leaf centre and its east /
+            // north unit vectors (zero at the poles, as the reference's guard)
+            float tl0 = 0.f, tl1 = 0.f, tl2 = 0.f, el0 = 0.f, el1 = 0.f, ep0 = 0.f, ep1 = 0.f, ep2 = 0.f;
+            if (rvalid) {
+                const double4 c = a.tgt[G.tgt + row];
+                tl0 = (float)(c.x - G.cx);
+                tl1 = (float)(c.y - G.cy);
+                tl2 = (float)(c.z - G.cz);
+                if ((fabs(c.z - 1.0) > 1e-15) && (fabs(c.z + 1.0) > 1e-15)) {
+                    const double omz = 1.0 - c.z * c.z, inv = 1.0 / sqrt(omz);
+                    el0 = (float)(-c.y * inv);
+                    el1 = (float)(c.x * inv);
+                    ep0 = (float)(-c.z * c.x * inv);
+                    ep1 = (float)(-c.z * c.y * inv);
+                    ep2 = (float)(omz * inv);
                 }
-                __syncwarp();
+            }
+            if (ni == 0) {
+                // no sources: the self pair alone
+                if (rvalid && ks == 0 && !*abort) {
+                    const int pos = G.tgt + row, idx = a.perm[pos];
+                    const double2 sk = a.selfk[pos];
+                    for (int f = 0; f < kF && a.f0 + f < a.nf; ++f) {
+                        const double w = (double)a.wF[(size_t)pos * kF + f];
+                        a.out_x[(size_t)(a.f0 + f) * a.ld_out + idx] = sk.x * w;
+                        a.out_y[(size_t)(a.f0 + f) * a.ld_out + idx] = sk.y * w;
+                    }
+                }
                 continue;
             }
-            if (use > 0) wait_bounded(&sm.empty[slot], (use - 1) & 1, abort, err);
-            float ve[4], vn[4];
+            int cur_slot = -1;
+            // the self pair (FP64 value / kernel constant, the weight carries the constant)
+            const int my_pos = G.tgt + row;
+            float self_e = 0.f, self_n = 0.f;
+            if (rvalid) {
+                const double2 sk = a.selfk[my_pos];
+                self_e = (float)sk.x;
+                self_n = (float)sk.y;
+            }
+            for (int k = 0; k < ni; ++k) {
+                const TcItem it = a.items[G.ib + k];
+                const int kind = it.kind & 3;
+                const int nst = (it.cnt + kStageK - 1) / kStageK;
+                if (kind == 2 && it.off != cur_slot) {
+                    // BLI bases of every target row in the new slot: thread
+                    // (row, 0) the xi basis, thread (row, 1) the eta basis
+                    cur_slot = it.off;
+                    producers_sync();
+                    if (rvalid) {
+                        const double2 e = a.xieta[G.tgt + row];
+                        const double *nodes = a.tgt_nodes + (size_t)it.off * 2 * n;
+                        if (ks == 0) down_basis(e.x, nodes, n, sm.fx[row]);
+                        else down_basis(e.y, nodes + n, n, sm.fe[row]);
+                    }
+                    producers_sync();
+                }
+                const float tx = tl0 - it.dx, ty = tl1 - it.dy, tz = tl2 - it.dz;
+                for (int j = 0; j < nst; ++j, ++st) {
+                    wait_slot(st);
+                    const uint32_t slot = st % kKStages;
+                    if (active) {
+                        float ve[8], vn[8];
+                        if (kind == 2) {
+                            // DOWN: BLI basis of the target x its unit vector's
+                            // component of the Cartesian row
+                            const int *km0 = sm.kmap + it.row0 + kStageK * j + 8 * ks;
+                            const float *fxr = sm.fx[row], *fer = sm.fe[row];
 #pragma unroll
-            for (int c = 0; c < 4; ++c) {
-                const int col = s * 8 + half * 4 + c;
-                if (it.kind == 2) {
-                    const int m = sm.kmap[it.mask + col];
-                    const float b = (col < cnt) ? sm.fx[row][m & 255] * sm.fe[row][(m >> 8) & 255] : 0.f;
-                    const int j = m >> 16;
-                    const float e = j == 0 ? el0 : el1;           // east z-component is 0
-                    const float np = j == 0 ? ep0 : (j == 1 ? ep1 : ep2);
-                    ve[c] = j == 2 ? 0.f : b * e;
-                    vn[c] = b * np;
-                } else {
-                    const float4 q = sm.loc[col];
-                    const float dx = q.x - tl0, dy = q.y - tl1, dz = q.z - tl2;
-                    const float v = val32(dx * dx + dy * dy + dz * dz);
-                    ve[c] = v * (el0 * dx + el1 * dy);
-                    vn[c] = v * (ep0 * dx + ep1 * dy + ep2 * dz);
+                            for (int c = 0; c < 8; ++c) {
+                                const int km = km0[c];
+                                const float b = fxr[km & 255] * fer[(km >> 8) & 255];
+                                const int comp = km >> 16;
+                                ve[c] = comp == 2 ? 0.f : b * (comp == 0 ? el0 : el1);
+                                vn[c] = b * (comp == 0 ? ep0 : (comp == 1 ? ep1 : ep2));
+                            }
+                        } else {
+                            // PP / PC: kernel value x projected displacement
+                            wait_bounded(&sm.wfull[st % kWStages], (st / kWStages) & 1, abort, err);
+                            const float4 *L = sm.loc[st % kWStages] + 8 * ks;
+#pragma unroll
+                            for (int c = 0; c < 8; ++c) {
+                                const float4 s4 = L[c];
+                                const float dx = s4.x - tx, dy = s4.y - ty, dz = s4.z - tz;
+                                const float v = val32(fmaf(dz, dz, fmaf(dy, dy, dx * dx)));
+                                ve[c] = v * fmaf(el1, dy, el0 * dx);
+                                vn[c] = v * fmaf(ep2, dz, fmaf(ep1, dy, ep0 * dx));
+                            }
+                            // the target itself among these 8 sources: the self pair
+                            const int cs = my_pos - (it.off + kStageK * j + 8 * ks);
+                            if (kind == 0 && (unsigned)cs < 8u) {
+#pragma unroll
+                                for (int c = 0; c < 8; ++c)
+                                    if (c == cs) { ve[c] = self_e; vn[c] = self_n; }
+                            }
+                        }
+                        // TF32 hi + lo (the tensor cores read lo's top 11 bits)
+                        float *th = sm.Kt[slot][ks][0], *tlo = sm.Kt[slot][ks][1];
+#pragma unroll
+                        for (int hh = 0; hh < 2; ++hh) {
+                            float4 eh, el, nh, nl;
+                            float *pe = &eh.x, *pel = &el.x, *pn = &nh.x, *pnl = &nl.x;
+#pragma unroll
+                            for (int c = 0; c < 4; ++c) {
+                                const float xe = ve[4 * hh + c], xn = vn[4 * hh + c];
+                                pe[c] = tf32_hi(xe);
+                                pel[c] = xe - pe[c];
+                                pn[c] = tf32_hi(xn);
+                                pnl[c] = xn - pn[c];
+                            }
+                            *reinterpret_cast<float4 *>(th + oe + 32 * hh) = eh;
+                            *reinterpret_cast<float4 *>(tlo + oe + 32 * hh) = el;
+                            *reinterpret_cast<float4 *>(th + on + 32 * hh) = nh;
+                            *reinterpret_cast<float4 *>(tlo + on + 32 * hh) = nl;
+                        }
+                        dev::fence_proxy_async();
+                    }
+                    __syncwarp();
+                    if (lane == 0) mbar_arrive(&sm.kfull[slot]);
                 }
             }
-            float4 eh, elo, nh, nlo;
-            split(ve[0], eh.x, elo.x);
-            split(ve[1], eh.y, elo.y);
-            split(ve[2], eh.z, elo.z);
-            split(ve[3], eh.w, elo.w);
-            split(vn[0], nh.x, nlo.x);
-            split(vn[1], nh.y, nlo.y);
-            split(vn[2], nh.z, nlo.z);
-            split(vn[3], nh.w, nlo.w);
-            const int ofs = canon(row, half * 4) >> 4;   // float4 index
-            sm.A[slot][0][ofs] = eh;
-            sm.A[slot][1][ofs] = elo;
-            sm.A[slot][2][ofs] = nh;
-            sm.A[slot][3][ofs] = nlo;
-            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            mbar_arrive(&sm.full[slot]);
         }
-    }
-    cp_wait0();
-    // ------------------------------------------------ epilogue
-    if (ni > 0 && producer) {
-        wait_bounded(&sm.item_done, (uint32_t)((ni - 1) & 1), abort, err);
-        tc_fence_after();
-        flush();
-    }
-    if (producer) {
-        // every thread takes part in the warp-wide tensor-memory loads; rows
-        // beyond the group's targets discard what they read
-        const bool write = rvalid && !*abort;
-        int idx = 0;
-        double self = 0.0, ar = 0.0;
-        double *out = half == 0 ? a.out_x : a.out_y;
-        if (write) {
-            const int pos = G.tgt + row;
-            idx = a.perm[pos];
-            const double4 c = a.tgt[pos];
-            dev::Tgt T;
-            dev::tgt_init(T, c.x, c.y, c.z);
-            double sx = 0.0, sy = 0.0;
-            if (T.live) dev::gref_exact(T, c.x, c.y, c.z, sx, sy);   // the self pair, in FP64
-            self = half == 0 ? sx : sy;
-            ar = a.area[pos];
-        }
-#pragma unroll
-        for (int cc = 0; cc < 4; ++cc) {
-            float y[16];
-            tmem_ld16(tmem + lane_base + run_col + 16 * cc, y);
-            tmem_wait_ld();
-            if (write) {
-#pragma unroll
-                for (int i = 0; i < 16; ++i) {
-                    const int f = a.f0 + 16 * cc + i;
-                    if (f < a.nf) {
-                        const double w = ar * a.ssh[(size_t)f * a.ld_ssh + idx];
-                        out[(size_t)f * a.ld_out + idx] = (double)y[i] + self * w;
+    } else if (warp == kMmaWarp) {
+        // ============================================================ MMA issue
+        uint32_t cc = 0;           // chains started
+        bool chain_open = false;
+        for (int gi = blockIdx.x; gi < a.ngroups; gi += gridDim.x) {
+            const MixGroup G = a.groups[gi];
+            for (int k = G.ib; k < G.ie; ++k) {
+                const TcItem it = a.items[k];
+                const int nst = (it.cnt + kStageK - 1) / kStageK;
+                for (int j = 0; j < nst; ++j, ++st) {
+                    const uint32_t slot = st % kKStages, jb = st % kWStages;
+                    wait_bounded(&sm.wfull[jb], (st / kWStages) & 1, abort, err);
+                    wait_bounded(&sm.kfull[slot], (st / kKStages) & 1, abort, err);
+                    // a new chain reuses the accumulator of chain cc - 2, which must be folded
+                    if (!chain_open && cc >= 2) wait_bounded(&sm.accfree[cc & 1], ((cc >> 1) - 1) & 1, abort, err);
+                    tc_fence_after();
+                    if (lane == 0) {
+                        if (!*abort) {
+                            const int nks = it.cnt - kStageK * j > 8 ? 2 : 1;
+                            for (int s = 0; s < nks; ++s) {
+                                const uint64_t aw = smem_desc(&sm.Wt[jb][s * kWStepFloats]);
+                                const uint64_t bh = smem_desc(sm.Kt[slot][s][0]), bl = smem_desc(sm.Kt[slot][s][1]);
+                                const uint32_t d = tmem + 256 * (cc & 1);
+                                mma_ss(d, aw, bh, (chain_open || s > 0) ? 1u : 0u);
+                                mma_ss(d, aw, bl, 1u);
+                            }
+                        }
+                        mma_commit(&sm.kempty[slot]);
+                        mma_commit(&sm.wempty[jb]);
                     }
+                    chain_open = true;
+                    __syncwarp();
                 }
+                if (it.kind & kTcFlush) {
+                    if (lane == 0) mma_commit(&sm.accfull[cc & 1]);
+                    __syncwarp();
+                    chain_open = false;
+                    ++cc;
+                }
+            }
+        }
+        // every MMA issued by this CTA completes before tensor memory is freed
+        if (lane == 0) {
+            mma_commit(&sm.fin);
+            wait_drain(&sm.fin, 0, err);
+        }
+        __syncwarp();
+    } else if (warp == kLoadWarp) {
+        // ============================================================ loads
+        for (int gi = blockIdx.x; gi < a.ngroups; gi += gridDim.x) {
+            const MixGroup G = a.groups[gi];
+            for (int k = G.ib; k < G.ie; ++k) {
+                const TcItem it = a.items[k];
+                const int nst = (it.cnt + kStageK - 1) / kStageK;
+                for (int j = 0; j < nst; ++j, ++st) {
+                    const uint32_t jb = st % kWStages, ub = st / kWStages;
+                    if (ub > 0) wait_bounded(&sm.wempty[jb], (ub - 1) & 1, abort, err);
+                    if (lane == 0) {
+                        const int ncol = min(kStageK, it.cnt - kStageK * j), nks = (ncol + 7) >> 3;
+                        const uint32_t wbytes = (uint32_t)nks * kWStepFloats * 4;
+                        const uint32_t lbytes = (it.kind & 3) != 2 ? (uint32_t)ncol * 16 : 0u;
+                        dev::mbar_expect_tx(&sm.wfull[jb], wbytes + lbytes);
+                        if (!*abort) {
+                            if (lbytes) dev::bulk_g2s(sm.loc[jb], a.sloc + it.off + kStageK * j, lbytes, &sm.wfull[jb]);
+                            dev::bulk_g2s(sm.Wt[jb], a.bstore + (size_t)(it.kb + 2 * j) * kWStepFloats, wbytes,
+                                          &sm.wfull[jb]);
+                        }
+                    }
+                    __syncwarp();
+                }
+            }
+        }
+        // no bulk copy may still be landing when the CTA exits
+        if (lane == 0)
+            for (uint32_t j = 0; j < (uint32_t)kWStages && j < st; ++j) {
+                const uint32_t uses = (st - 1 - j) / kWStages + 1;
+                wait_drain(&sm.wfull[j], (uses - 1) & 1, err);
+            }
+        __syncwarp();
+    }
+    else {
+        // ============================================================ folds
+        const int q = warp & 3;
+        const uint32_t tq = tmem + ((uint32_t)(32 * q) << 16);
+        uint32_t cc = 0;   // chains folded
+        for (int gi = blockIdx.x; gi < a.ngroups; gi += gridDim.x) {
+            const MixGroup G = a.groups[gi];
+            bool first = true;
+            for (int k = G.ib; k < G.ie; ++k) {
+                if (!(a.items[k].kind & kTcFlush)) continue;
+                wait_bounded(&sm.accfull[cc & 1], (cc >> 1) & 1, abort, err);
+                tc_fence_after();
+                fold_chain(tq + 256 * (cc & 1), &sm.run[0][0], q, lane, k == G.ie - 1, first, G.tgt, G.nt, a.perm,
+                           a.out_x, a.out_y, a.ld_out, a.f0, a.nf, *abort != 0);
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&sm.accfree[cc & 1]);
+                first = false;
+                ++cc;
             }
         }
     }
@@ -424,13 +517,88 @@ __global__ void __launch_bounds__(kThreads, 2) tc_leaf_kernel(MixArgs a, int *er
     }
 }
 
-size_t tc_smem_bytes() { return sizeof(TcSmem) + 1024; }
+// Split weight store: per k-step of 8 store rows, the 64-field rows as one
+// 128-row TF32 tile (field f's hi part at row wrow(f, 0), lo part at
+// wrow(f, 1)) in the canonical no-swizzle K-major layout.  One thread per
+// (k-step, field).
+__global__ void split_store_kernel(const int32_t *__restrict__ bsrc, int64_t nk, const float *__restrict__ wF,
+                                   const float *__restrict__ phiF, float *__restrict__ bstore) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nk * kF) return;
+    const int64_t ks = t / kF;
+    const int f = (int)(t % kF);
+    float hi[8], lo[8];
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+        const int32_t s = bsrc[ks * 8 + r];
+        const float v = s >= 0 ? wF[(size_t)s * kF + f] : (s <= -2 ? phiF[(size_t)(-2 - s) * kF + f] : 0.f);
+        hi[r] = tf32_hi(v);
+        lo[r] = tf32_hi(v - hi[r]);
+    }
+    float *base = bstore + ks * kWStepFloats;
+    const int oh = canon(wrow(f, 0), 0) >> 2, ol = canon(wrow(f, 1), 0) >> 2;
+    *reinterpret_cast<float4 *>(base + oh) = make_float4(hi[0], hi[1], hi[2], hi[3]);
+    *reinterpret_cast<float4 *>(base + oh + 32) = make_float4(hi[4], hi[5], hi[6], hi[7]);
+    *reinterpret_cast<float4 *>(base + ol) = make_float4(lo[0], lo[1], lo[2], lo[3]);
+    *reinterpret_cast<float4 *>(base + ol + 32) = make_float4(lo[4], lo[5], lo[6], lo[7]);
+}
 
-void launch_tc_leaf(const MixArgs &a, int ngroups, int *err, cudaStream_t st) {
-    if (ngroups <= 0) return;
+// Per pool row, the FP32 coordinates relative to the centre of the row's own
+// panel (a leaf for points, the slot panel for proxies).  One block per range.
+__global__ void source_local_kernel(const double4 *__restrict__ pool, const int2 *__restrict__ ranges,
+                                    const double4 *__restrict__ centres, float4 *__restrict__ sloc) {
+    const int2 r = ranges[blockIdx.x];
+    const double4 c = centres[blockIdx.x];
+    for (int p = r.x + threadIdx.x; p < r.y; p += blockDim.x) {
+        const double4 s = pool[p];
+        sloc[p] = make_float4((float)(s.x - c.x), (float)(s.y - c.y), (float)(s.z - c.z), 0.f);
+    }
+}
+
+// Per pool point, the self pair of sal_grad_gfunc (fast_sum_module.f90:9-31)
+// in FP64 divided by the kernel constant: the leaf epilogue multiplies it by
+// the point's FP32 weight row, which carries the constant.
+__global__ void self_pair_kernel(const double4 *__restrict__ pool, int n, double2 *__restrict__ selfk) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    const double4 c = pool[p];
+    dev::Tgt T;
+    dev::tgt_init(T, c.x, c.y, c.z);
+    double sx = 0.0, sy = 0.0;
+    if (T.live) dev::gref_exact(T, c.x, c.y, c.z, sx, sy);
+    selfk[p] = make_double2(sx / dev::kCons, sy / dev::kCons);
+}
+
+size_t tc_smem_bytes() {
+    // above half of the SM's shared memory: one CTA per SM, which owns all
+    // 512 tensor memory columns
+    const size_t need = sizeof(TcSmem) + 1024;
+    return need > 120 * 1024 ? need : 120 * 1024;
+}
+
+void launch_tc_leaf(const TcArgs &a, int nsm, int *err, cudaStream_t st) {
+    if (a.ngroups <= 0) return;
     const size_t smem = tc_smem_bytes();
     cudaFuncSetAttribute(tc_leaf_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    tc_leaf_kernel<<<ngroups, kThreads, smem, st>>>(a, err);
+    const int grid = a.ngroups < nsm ? a.ngroups : nsm;
+    tc_leaf_kernel<<<grid, kThreads, smem, st>>>(a, err);
+}
+
+void launch_split_store(const int32_t *bsrc, int64_t nrows, const float *wF, const float *phiF, float *bstore,
+                        cudaStream_t st) {
+    const int64_t nk = nrows / 8;
+    if (nk <= 0) return;
+    const int64_t threads = nk * kF;
+    split_store_kernel<<<(unsigned)((threads + 255) / 256), 256, 0, st>>>(bsrc, nk, wF, phiF, bstore);
+}
+
+void launch_source_local(const double4 *pool, const int2 *ranges, const double4 *centres, int nranges, float4 *sloc,
+                         cudaStream_t st) {
+    if (nranges > 0) source_local_kernel<<<nranges, 128, 0, st>>>(pool, ranges, centres, sloc);
+}
+
+void launch_self_pair(const double4 *pool, int n, double2 *selfk, cudaStream_t st) {
+    if (n > 0) self_pair_kernel<<<(n + 255) / 256, 256, 0, st>>>(pool, n, selfk);
 }
 
 }  // namespace mix
