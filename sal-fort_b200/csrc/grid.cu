@@ -64,6 +64,7 @@ struct GridImpl {
     int32_t *bsrc = nullptr;
     float *bstore = nullptr;          // split weight store of the tcgen05 leaf pass
     float4 *sloc = nullptr;
+    float *sxyz = nullptr;
     double2 *selfk = nullptr;
     int nsm = 0;
     Item *mix_leaf_items = nullptr, *mix_proxy_items = nullptr;
@@ -364,6 +365,7 @@ static int ensure_mixed(GridImpl &g, int FT) {
         if (!rc) rc = dalloc(g, &g.bstore, pl.bsrc.size() * 2 * (size_t)FT);
         if (!rc) rc = dalloc(g, &g.sloc, n + (size_t)g.nsrc * P);
         if (!rc) rc = dalloc(g, &g.selfk, n);
+        if (!rc) rc = dalloc(g, &g.sxyz, (size_t)pl.tc_src_ksteps * 24);
         if (!rc) {
             const size_t nr = pl.sloc_ranges.size() / 2;
             std::vector<int2> ranges(nr);
@@ -381,6 +383,7 @@ static int ensure_mixed(GridImpl &g, int FT) {
             if (e == cudaSuccess) {
                 mix::launch_source_local(g.pool, dr, dc, (int)ranges.size(), g.sloc, g.stream);
                 mix::launch_self_pair(g.pool, (int)n, g.selfk, g.stream);
+                mix::launch_source_ksteps(g.bsrc, pl.tc_src_ksteps, g.sloc, g.sxyz, g.stream);
                 e = cudaStreamSynchronize(g.stream);
             }
             cudaFree(dr);
@@ -448,7 +451,7 @@ static void solve_mixed_block(GridImpl &g, const double *ssh, int64_t ld_ssh, in
         t.groups = g.tc_leaf_groups;
         t.ngroups = (int)pl.tc_leaf_groups.size();
         t.items = g.tc_items;
-        t.sloc = g.sloc;
+        t.sxyz = g.sxyz;
         t.bstore = g.bstore;
         t.tgt = g.pool;
         t.xieta = g.xieta;

@@ -39,7 +39,7 @@ struct TcArgs {
     const MixGroup *groups;   // leaf groups of <= 128 targets, pool order
     int ngroups;
     const TcItem *items;
-    const float4 *sloc;       // per pool row: coordinates relative to the row's panel centre
+    const float *sxyz;        // per source k-step of the split store: x[8], y[8], z[8] relative to the panel centre
     const float *bstore;      // split weight store: 1024 floats per k-step of 8 rows
     const double4 *tgt;       // pool (targets are its first n rows)
     const double2 *xieta;     // per pool position
@@ -59,6 +59,7 @@ void launch_split_store(const int32_t *bsrc, int64_t nrows, const float *wF, con
 void launch_source_local(const double4 *pool, const int2 *ranges, const double4 *centres, int nranges, float4 *sloc,
                          cudaStream_t st);
 void launch_self_pair(const double4 *pool, int n, double2 *selfk, cudaStream_t st);
+void launch_source_ksteps(const int32_t *bsrc, int64_t nks, const float4 *sloc, float *sxyz, cudaStream_t st);
 
 }  // namespace mix
 }  // namespace sal

@@ -371,6 +371,7 @@ bool plan_build(const Tree &t, int d, int mode, const int32_t *list, int64_t nli
         const int64_t src_b0 = nb, P8 = up8(P), P38 = up8(3 * P);
         nb += (int64_t)nsrc * P8;
         const int64_t phi_b0 = nb;
+        pl->tc_src_ksteps = phi_b0 / 8;
         nb += (int64_t)ntgt * P38;
         if (nb / 8 > INT32_MAX / 2) { *err = "grid too large for the split weight store"; return false; }
         pl->bsrc.assign((size_t)nb, -1);

@@ -129,6 +129,7 @@ struct Plan {
     std::vector<MixGroup> tc_leaf_groups;
     std::vector<TcItem> tc_items;
     std::vector<int32_t> bsrc;
+    int64_t tc_src_ksteps = 0;                    // k-steps of the store holding sources (points, proxies)
     // pool row ranges (begin, end) of every leaf and every source slot's
     // proxies, with the centre (x, y, z) of the range's panel
     std::vector<int32_t> sloc_ranges;

@@ -21,7 +21,9 @@
 //   warp 8      issues the MMAs.
 //   warp 9      loads, per stage, the weight tiles (pre-split TF32 hi / lo,
 //               written once per solve by split_store_kernel) and the sources'
-//               FP32 coordinates with bulk copies into a 4-deep ring.
+//               FP32 coordinates (per k-step x[8] y[8] z[8], so that column
+//               pairs load as float2 for the packed FP32x2 arithmetic) with
+//               bulk copies into a 4-deep ring.
 //   warps 10-13 fold finished accumulator chains into the running sums and
 //               write the outputs (warp w: tensor memory lanes 32(w%4)..+31).
 // The tensor cores accumulate with truncation, so one chain over all of a
@@ -70,7 +72,7 @@ constexpr uint32_t kIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(256
 struct TcSmem {
     float Kt[kKStages][2][2][kTileFloats];       // per stage: k-step x {hi, lo} x 256 rows x 8
     float Wt[kWStages][2 * kWStepFloats];        // per stage: 2 k-steps x 128 weight rows x 8
-    float4 loc[kWStages][kStageK];               // per stage: source coordinates of its 16 columns
+    float lxyz[kWStages][2][24];                 // per stage and k-step: source x[8], y[8], z[8]
     float run[2 * kTcRows][kF];                  // running sums: [component x target][field, 16-blocks swapped on odd targets]
     float fx[kTcRows][kMaxDegree + 1];           // per target row: BLI bases in the current DOWN slot
     float fe[kTcRows][kMaxDegree + 1];
@@ -80,17 +82,25 @@ struct TcSmem {
     int abort;
 };
 
-__device__ __forceinline__ float val32(float mp) {
-    // mp = 0 only for a source on the target itself (or a repeated point),
-    // where the projected displacement is exactly 0: the clamp keeps the
-    // value finite so that the entry is 0.
-    mp = fmaxf(mp, 1e-20f);
-    float r, u;
-    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(mp));
-    const float q = mp * r;
-    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(u) : "f"(2.f + q));
-    const float inner = fmaf(kC1F, r, fmaf(kTwoC2F, u, -kTwoC2F));
-    return inner * r * r;
+
+// Packed FP32x2 arithmetic (two kernel-tile columns per instruction).
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) {
+    unsigned long long r;
+    asm("sub.rn.f32x2 %0, %1, %2;"
+        : "=l"(r)
+        : "l"(*reinterpret_cast<unsigned long long *>(&a)), "l"(*reinterpret_cast<unsigned long long *>(&b)));
+    return *reinterpret_cast<float2 *>(&r);
+}
+__device__ __forceinline__ float2 f2(float x) { return make_float2(x, x); }
+__device__ __forceinline__ float rsqrt_approx(float x) {
+    float r;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+__device__ __forceinline__ float rcp_approx(float x) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
 }
 
 __device__ __forceinline__ float tf32_hi(float x) {
@@ -188,6 +198,40 @@ __host__ __device__ constexpr int wrow(int f, int part) { return 32 * (f >> 4) +
 // 16-31 the odd one, so hi + lo of a field meet in one lane.  Mid-group:
 // running sum (+)= chain (the group's first chain stores).  At the group's
 // end: running sum + chain to the caller's outputs for its nt targets.
+// Tensor memory loads are double-buffered and each 16-column chunk reads its
+// 8 running-sum entries before it writes any, so the chunk's latencies overlap.
+__device__ __forceinline__ void fold_chunk(const float (&x)[16], int c0, float *run, int f, int odd, bool end,
+                                           bool first, int nt, int idk, double *out, int64_t ld_out, bool wr) {
+    float v[8], rs[8];
+    float *rp[8];
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+        const float lo_even = __shfl_down_sync(0xffffffffu, x[2 * m], 16);
+        const float hi_odd = __shfl_up_sync(0xffffffffu, x[2 * m + 1], 16);
+        v[m] = odd ? x[2 * m + 1] + hi_odd : x[2 * m] + lo_even;
+        // odd target slots store their fields with the 16-blocks swapped,
+        // so the two half-warps hit different banks
+        rp[m] = run + (size_t)(c0 + 2 * m + odd) * kF + (f ^ (odd << 4));
+    }
+    if (!first) {
+#pragma unroll
+        for (int m = 0; m < 8; ++m) rs[m] = *rp[m];
+#pragma unroll
+        for (int m = 0; m < 8; ++m) v[m] += rs[m];
+    }
+    if (!end) {
+#pragma unroll
+        for (int m = 0; m < 8; ++m) *rp[m] = v[m];
+    } else {
+#pragma unroll
+        for (int m = 0; m < 8; ++m) {
+            const int t = (c0 & 127) + 2 * m + odd;
+            const int ti = __shfl_sync(0xffffffffu, idk, t & 31);
+            if (wr && t < nt) out[ti] = (double)v[m];
+        }
+    }
+}
+
 __device__ __noinline__ void fold_chain(uint32_t td, float *run, int q, int lane, bool end, bool first, int tgt,
                                         int nt, const int32_t *__restrict__ perm, double *out_x, double *out_y,
                                         int64_t ld_out, int f0, int nf, bool skip) {
@@ -196,31 +240,30 @@ __device__ __noinline__ void fold_chain(uint32_t td, float *run, int q, int lane
     if (end)
 #pragma unroll
         for (int k = 0; k < 4; ++k) idx[k] = 32 * k + lane < nt ? perm[tgt + 32 * k + lane] : 0;
+    const bool wr = end && f0 + f < nf && !skip;
+    double *ox = out_x + (size_t)(f0 + f) * ld_out, *oy = out_y + (size_t)(f0 + f) * ld_out;
+    // chunks of 16 columns: component ch = c / 128, target slots c % 128 ..+15;
+    // at a group's end only the chunks that hold targets
+    const int per = end ? (nt + 15) / 16 : 8;
+    const int nchunk = 2 * per;
+    auto col = [&](int i) { return (i / per) * 128 + (i % per) * 16; };
+    float xa[16], xb[16];
+    tmem_ld16(td + col(0), xa);
 #pragma unroll 1
-    for (int cc = 0; cc < 256; cc += 16) {
-        const int ch = cc >> 7, c0 = cc & 127;
-        if (end && c0 >= nt) continue;
-        float x[16];
-        tmem_ld16(td + cc, x);
+    for (int i = 0; i < nchunk; i += 2) {
         tmem_wait_ld();
-        const int ik = c0 >> 5;
-        const int idk = ik == 0 ? idx[0] : ik == 1 ? idx[1] : ik == 2 ? idx[2] : idx[3];
-        double *out = ch == 0 ? out_x : out_y;
-#pragma unroll
-        for (int m = 0; m < 8; ++m) {
-            const float lo_even = __shfl_down_sync(0xffffffffu, x[2 * m], 16);
-            const float hi_odd = __shfl_up_sync(0xffffffffu, x[2 * m + 1], 16);
-            const float v = odd ? x[2 * m + 1] + hi_odd : x[2 * m] + lo_even;
-            const int t = c0 + 2 * m + odd;                 // target slot
-            // odd target slots store their fields with the 16-blocks swapped,
-            // so the two half-warps hit different banks
-            float *rp = run + (size_t)(128 * ch + t) * kF + (f ^ (odd << 4));
-            const float sum = first ? v : *rp + v;
-            const int ti = __shfl_sync(0xffffffffu, idk, t & 31);
-            if (!end)
-                *rp = sum;
-            else if (t < nt && f0 + f < nf && !skip)
-                out[(size_t)(f0 + f) * ld_out + ti] = (double)sum;
+        if (i + 1 < nchunk) tmem_ld16(td + col(i + 1), xb);
+        {
+            const int c = col(i), ik = (c & 127) >> 5;
+            const int idk = ik == 0 ? idx[0] : ik == 1 ? idx[1] : ik == 2 ? idx[2] : idx[3];
+            fold_chunk(xa, c, run, f, odd, end, first, nt, idk, c < 128 ? ox : oy, ld_out, wr);
+        }
+        if (i + 1 < nchunk) {
+            tmem_wait_ld();
+            if (i + 2 < nchunk) tmem_ld16(td + col(i + 2), xa);
+            const int c = col(i + 1), ik = (c & 127) >> 5;
+            const int idk = ik == 0 ? idx[0] : ik == 1 ? idx[1] : ik == 2 ? idx[2] : idx[3];
+            fold_chunk(xb, c, run, f, odd, end, first, nt, idk, c < 128 ? ox : oy, ld_out, wr);
         }
     }
 }
@@ -262,9 +305,6 @@ __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(TcArgs a, int *err
         const int p = kk / 3;
         sm.kmap[k] = (p % n) | ((p / n) << 8) | ((kk % 3) << 16);
     }
-    // columns past an item's sources read these until a copy overwrites them
-    for (int k = tid; k < kWStages * kStageK; k += kThreads)
-        sm.loc[k / kStageK][k % kStageK] = make_float4(4.f, 4.f, 4.f, 0.f);
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
@@ -316,6 +356,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(TcArgs a, int *err
                 }
                 continue;
             }
+            const float2 el0v = f2(el0), el1v = f2(el1), ep0v = f2(ep0), ep1v = f2(ep1), ep2v = f2(ep2);
             int cur_slot = -1;
             // the self pair (FP64 value / kernel constant, the weight carries the constant)
             const int my_pos = G.tgt + row;
@@ -342,7 +383,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(TcArgs a, int *err
                     }
                     producers_sync();
                 }
-                const float tx = tl0 - it.dx, ty = tl1 - it.dy, tz = tl2 - it.dz;
+                const float2 tx2 = f2(tl0 - it.dx), ty2 = f2(tl1 - it.dy), tz2 = f2(tl2 - it.dz);
                 for (int j = 0; j < nst; ++j, ++st) {
                     wait_slot(st);
                     const uint32_t slot = st % kKStages;
@@ -362,16 +403,32 @@ __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(TcArgs a, int *err
                                 vn[c] = b * (comp == 0 ? ep0 : (comp == 1 ? ep1 : ep2));
                             }
                         } else {
-                            // PP / PC: kernel value x projected displacement
+                            // PP / PC: kernel value x projected displacement,
+                            // two columns per packed instruction
                             wait_bounded(&sm.wfull[st % kWStages], (st / kWStages) & 1, abort, err);
-                            const float4 *L = sm.loc[st % kWStages] + 8 * ks;
+                            const float *L = sm.lxyz[st % kWStages][ks];
 #pragma unroll
-                            for (int c = 0; c < 8; ++c) {
-                                const float4 s4 = L[c];
-                                const float dx = s4.x - tx, dy = s4.y - ty, dz = s4.z - tz;
-                                const float v = val32(fmaf(dz, dz, fmaf(dy, dy, dx * dx)));
-                                ve[c] = v * fmaf(el1, dy, el0 * dx);
-                                vn[c] = v * fmaf(ep2, dz, fmaf(ep1, dy, ep0 * dx));
+                            for (int c2 = 0; c2 < 4; ++c2) {
+                                const float2 dx = sub2(*reinterpret_cast<const float2 *>(L + 2 * c2), tx2);
+                                const float2 dy = sub2(*reinterpret_cast<const float2 *>(L + 8 + 2 * c2), ty2);
+                                const float2 dz = sub2(*reinterpret_cast<const float2 *>(L + 16 + 2 * c2), tz2);
+                                float2 mp = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
+                                // mp = 0 only for a source on the target itself (or a
+                                // repeated point): the clamp keeps the value finite
+                                mp.x = fmaxf(mp.x, 1e-20f);
+                                mp.y = fmaxf(mp.y, 1e-20f);
+                                const float2 r = make_float2(rsqrt_approx(mp.x), rsqrt_approx(mp.y));
+                                const float2 w = __fadd2_rn(__fmul2_rn(mp, r), f2(2.f));
+                                const float2 u = make_float2(rcp_approx(w.x), rcp_approx(w.y));
+                                const float2 inner = __ffma2_rn(f2(kC1F), r, __ffma2_rn(f2(kTwoC2F), u, f2(-kTwoC2F)));
+                                const float2 v = __fmul2_rn(inner, __fmul2_rn(r, r));
+                                const float2 pe = __ffma2_rn(el1v, dy, __fmul2_rn(el0v, dx));
+                                const float2 pn = __ffma2_rn(ep2v, dz, __ffma2_rn(ep1v, dy, __fmul2_rn(ep0v, dx)));
+                                const float2 e2 = __fmul2_rn(v, pe), n2 = __fmul2_rn(v, pn);
+                                ve[2 * c2] = e2.x;
+                                ve[2 * c2 + 1] = e2.y;
+                                vn[2 * c2] = n2.x;
+                                vn[2 * c2 + 1] = n2.y;
                             }
                             // the target itself among these 8 sources: the self pair
                             const int cs = my_pos - (it.off + kStageK * j + 8 * ks);
@@ -385,20 +442,18 @@ __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(TcArgs a, int *err
                         float *th = sm.Kt[slot][ks][0], *tlo = sm.Kt[slot][ks][1];
 #pragma unroll
                         for (int hh = 0; hh < 2; ++hh) {
-                            float4 eh, el, nh, nl;
-                            float *pe = &eh.x, *pel = &el.x, *pn = &nh.x, *pnl = &nl.x;
-#pragma unroll
-                            for (int c = 0; c < 4; ++c) {
-                                const float xe = ve[4 * hh + c], xn = vn[4 * hh + c];
-                                pe[c] = tf32_hi(xe);
-                                pel[c] = xe - pe[c];
-                                pn[c] = tf32_hi(xn);
-                                pnl[c] = xn - pn[c];
-                            }
+                            const float4 eh = make_float4(tf32_hi(ve[4 * hh]), tf32_hi(ve[4 * hh + 1]),
+                                                          tf32_hi(ve[4 * hh + 2]), tf32_hi(ve[4 * hh + 3]));
+                            const float4 nh = make_float4(tf32_hi(vn[4 * hh]), tf32_hi(vn[4 * hh + 1]),
+                                                          tf32_hi(vn[4 * hh + 2]), tf32_hi(vn[4 * hh + 3]));
+                            const float2 el01 = sub2(make_float2(ve[4 * hh], ve[4 * hh + 1]), make_float2(eh.x, eh.y));
+                            const float2 el23 = sub2(make_float2(ve[4 * hh + 2], ve[4 * hh + 3]), make_float2(eh.z, eh.w));
+                            const float2 nl01 = sub2(make_float2(vn[4 * hh], vn[4 * hh + 1]), make_float2(nh.x, nh.y));
+                            const float2 nl23 = sub2(make_float2(vn[4 * hh + 2], vn[4 * hh + 3]), make_float2(nh.z, nh.w));
                             *reinterpret_cast<float4 *>(th + oe + 32 * hh) = eh;
-                            *reinterpret_cast<float4 *>(tlo + oe + 32 * hh) = el;
+                            *reinterpret_cast<float4 *>(tlo + oe + 32 * hh) = make_float4(el01.x, el01.y, el23.x, el23.y);
                             *reinterpret_cast<float4 *>(th + on + 32 * hh) = nh;
-                            *reinterpret_cast<float4 *>(tlo + on + 32 * hh) = nl;
+                            *reinterpret_cast<float4 *>(tlo + on + 32 * hh) = make_float4(nl01.x, nl01.y, nl23.x, nl23.y);
                         }
                         dev::fence_proxy_async();
                     }
@@ -467,10 +522,11 @@ __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(TcArgs a, int *err
                     if (lane == 0) {
                         const int ncol = min(kStageK, it.cnt - kStageK * j), nks = (ncol + 7) >> 3;
                         const uint32_t wbytes = (uint32_t)nks * kWStepFloats * 4;
-                        const uint32_t lbytes = (it.kind & 3) != 2 ? (uint32_t)ncol * 16 : 0u;
+                        const uint32_t lbytes = (it.kind & 3) != 2 ? (uint32_t)nks * 96 : 0u;
                         dev::mbar_expect_tx(&sm.wfull[jb], wbytes + lbytes);
                         if (!*abort) {
-                            if (lbytes) dev::bulk_g2s(sm.loc[jb], a.sloc + it.off + kStageK * j, lbytes, &sm.wfull[jb]);
+                            if (lbytes)
+                                dev::bulk_g2s(sm.lxyz[jb], a.sxyz + (size_t)(it.kb + 2 * j) * 24, lbytes, &sm.wfull[jb]);
                             dev::bulk_g2s(sm.Wt[jb], a.bstore + (size_t)(it.kb + 2 * j) * kWStepFloats, wbytes,
                                           &sm.wfull[jb]);
                         }
@@ -555,6 +611,21 @@ __global__ void source_local_kernel(const double4 *__restrict__ pool, const int2
     }
 }
 
+// Source coordinates per k-step of the split store: x[8], y[8], z[8] of its
+// rows (a far dummy point for padding rows, which carry zero weights).
+__global__ void source_ksteps_kernel(const int32_t *__restrict__ bsrc, int64_t nks, const float4 *__restrict__ sloc,
+                                     float *__restrict__ sxyz) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nks * 8) return;
+    const int64_t ks = t >> 3;
+    const int i = (int)(t & 7);
+    const int32_t r = bsrc[t];
+    const float4 p = r >= 0 ? sloc[r] : make_float4(4.f, 4.f, 4.f, 0.f);
+    sxyz[ks * 24 + i] = p.x;
+    sxyz[ks * 24 + 8 + i] = p.y;
+    sxyz[ks * 24 + 16 + i] = p.z;
+}
+
 // Per pool point, the self pair of sal_grad_gfunc (fast_sum_module.f90:9-31)
 // in FP64 divided by the kernel constant: the leaf epilogue multiplies it by
 // the point's FP32 weight row, which carries the constant.
@@ -595,6 +666,10 @@ void launch_split_store(const int32_t *bsrc, int64_t nrows, const float *wF, con
 void launch_source_local(const double4 *pool, const int2 *ranges, const double4 *centres, int nranges, float4 *sloc,
                          cudaStream_t st) {
     if (nranges > 0) source_local_kernel<<<nranges, 128, 0, st>>>(pool, ranges, centres, sloc);
+}
+
+void launch_source_ksteps(const int32_t *bsrc, int64_t nks, const float4 *sloc, float *sxyz, cudaStream_t st) {
+    if (nks > 0) source_ksteps_kernel<<<(unsigned)((nks * 8 + 255) / 256), 256, 0, st>>>(bsrc, nks, sloc, sxyz);
 }
 
 void launch_self_pair(const double4 *pool, int n, double2 *selfk, cudaStream_t st) {
