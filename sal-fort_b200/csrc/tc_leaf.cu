@@ -1,7 +1,7 @@
 // Leaf pass of the batched form on the 5th-generation tensor cores (tcgen05).
 //
-// Persistent kernel, one CTA per SM, walking leaf groups of up to 128 targets
-// in pool order with a stride of the grid size.  A group's work is a list of
+// One CTA per SM at a time, each walking a few leaf groups of up to 128
+// targets in pool order with a stride of the grid size.  A group's work is a list of
 // items (<= 64 sources, or <= 64 Cartesian rows of a DOWN interpolation), cut
 // into stages of 16 K columns (two k-steps of 8).  The contraction is
 //     D[field part, target component] += W[field part, k] * T[k, target component]
@@ -55,6 +55,7 @@ constexpr int kF = 64;                            // fields
 constexpr int kStageK = 16;                       // K columns per stage (two k-steps of 8)
 constexpr int kKStages = 3;                       // kernel-tile ring
 constexpr int kWStages = 4;                       // weight / coordinate ring
+constexpr int kMaxGroupsPerCta = 4;               // CTAs stay short (see launch_tc_leaf)
 constexpr int kTileFloats = 2048;                 // kernel tile of one k-step: 256 rows x 8, one of hi / lo
 constexpr int kWStepFloats = 1024;                // weight tile of one k-step: 128 rows x 8
 constexpr int kTmemCols = 512;
@@ -651,7 +652,10 @@ void launch_tc_leaf(const TcArgs &a, int nsm, int *err, cudaStream_t st) {
     if (a.ngroups <= 0) return;
     const size_t smem = tc_smem_bytes();
     cudaFuncSetAttribute(tc_leaf_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    const int grid = a.ngroups < nsm ? a.ngroups : nsm;
+    // every SM busy, but no CTA longer than kMaxGroupsPerCta groups, so that
+    // kernels of other streams (higher-priority grids) get SMs as CTAs retire
+    int grid = (a.ngroups + kMaxGroupsPerCta - 1) / kMaxGroupsPerCta;
+    if (grid < nsm) grid = a.ngroups < nsm ? a.ngroups : nsm;
     tc_leaf_kernel<<<grid, kThreads, smem, st>>>(a, err);
 }
 

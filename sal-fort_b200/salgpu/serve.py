@@ -5,7 +5,13 @@ time (code.f90).  Here each registered grid keeps its tree, interaction lists,
 proxies and work plan resident in device memory; SSH fields arrive as
 requests (1..64 fields each), are batched per grid as they arrive, and each
 batch is one batched mixed-precision solve (SAL_FORM_MIXED) on the grid's own
-CUDA stream, so batches of different grids overlap on the device.
+CUDA stream, so batches of different grids overlap on the device.  Smaller
+grids get higher stream priorities: their short batches are scheduled onto
+SMs ahead of a large grid's long one as its CTAs retire.
+
+A request's fields are either a host array (copied through the grid's pinned
+staging buffers; results come back as host arrays) or a CUDA tensor on the
+server's device (copied device to device; results stay on the device).
 
 Scheduling rules:
   * a grid has at most one batch in flight (its batch buffers are its own);
@@ -17,8 +23,8 @@ Scheduling rules:
     refused and its requests fail with `SalError(SAL_ENOMEM)`;
   * requests can be cancelled until their batch is launched.
 
-Latency of a request = completion of its batch's device-to-host copy minus
-its arrival time.  Each field's result does not depend on which other fields
+Latency of a request = completion of its batch (including the copy of its
+results into its own arrays) minus its arrival time.  Each field's result does not depend on which other fields
 share its batch (tensor-core columns never mix), which
 tests/test_serve.py checks.
 """
@@ -37,12 +43,12 @@ from . import FORM_MIXED, MODE_DTT, SAL_EINVAL, SAL_ENOMEM, Grid, SalError, dual
 @dataclass
 class Request:
     grid: str
-    ssh: np.ndarray            # (F, N) float64, host
+    ssh: object                # (F, N) float64: numpy array (host) or CUDA tensor (device)
     arrival: float = 0.0
     rid: int = -1
     status: str = "pending"    # pending | running | done | failed | cancelled
-    out_x: np.ndarray | None = None
-    out_y: np.ndarray | None = None
+    out_x: object = None         # same kind as ssh
+    out_y: object = None
     error: Exception | None = None
     done_time: float = 0.0
 
@@ -85,13 +91,14 @@ class _Resident:
     inflight: list | None = None
     event: object = None
     last_used: float = 0.0
+    launched: float = 0.0
 
 
 class Server:
     """Resident grids + per-grid continuous batching on CUDA streams."""
 
     def __init__(self, hbm_budget_bytes: int, max_batch: int = 64, device: int = 0, clock=time.perf_counter,
-                 grid_factory=Grid):
+                 grid_factory=Grid, priorities: bool = True):
         try:
             import torch
         except ImportError:           # the CPU test double needs no torch
@@ -107,6 +114,8 @@ class Server:
         self._ids = itertools.count()
         self.completed: list[Request] = []
         self.evictions = 0
+        self.priorities = priorities
+        self.batches: list[tuple] = []     # (grid, fields, launch time, done time) of finished batches
 
     # ------------------------------------------------------------------ grids
     def register_grid(self, spec: GridSpec) -> None:
@@ -156,12 +165,20 @@ class Server:
 
     # ------------------------------------------------------------------ device hooks
     # (a test double overrides these four to exercise the scheduling on the CPU)
+    def _stream_priority(self, r: _Resident) -> int:
+        # rank of the grid by size among the registered grids: the smallest
+        # gets the highest priority (most negative); torch clamps to the range
+        if not self.priorities:
+            return 0
+        sizes = sorted({len(g.spec.xs) for g in self.grids.values()})
+        return -(len(sizes) - 1 - sizes.index(len(r.spec.xs)))
+
     def _alloc_staging(self, r: _Resident) -> None:
         torch = self.torch
         n = len(r.spec.xs)
         dev = torch.device("cuda", self.device)
         if r.stream is None:
-            r.stream = torch.cuda.Stream(device=dev)
+            r.stream = torch.cuda.Stream(device=dev, priority=self._stream_priority(r))
             r.h_in = torch.empty((self.max_batch, n), dtype=torch.float64).pin_memory()
             r.h_ox = torch.empty((self.max_batch, n), dtype=torch.float64).pin_memory()
             r.h_oy = torch.empty((self.max_batch, n), dtype=torch.float64).pin_memory()
@@ -171,25 +188,43 @@ class Server:
 
     def _launch_device(self, r: _Resident, batch: list, nf: int) -> None:
         torch = self.torch
+        on_dev = [isinstance(q.ssh, torch.Tensor) for q in batch]
         f = 0
-        for q in batch:
-            r.h_in[f:f + q.nfields].numpy()[:] = q.ssh
+        for q, d in zip(batch, on_dev):
+            if not d:
+                r.h_in[f:f + q.nfields].numpy()[:] = q.ssh
             f += q.nfields
+        # device requests were written on the submitting thread's stream
+        r.stream.wait_stream(torch.cuda.current_stream(r.ssh_dev.device))
         with torch.cuda.stream(r.stream):
-            r.ssh_dev[:nf].copy_(r.h_in[:nf], non_blocking=True)
+            f = 0
+            for q, d in zip(batch, on_dev):
+                src = q.ssh if d else r.h_in[f:f + q.nfields]
+                r.ssh_dev[f:f + q.nfields].copy_(src, non_blocking=True)
+                f += q.nfields
             r.grid.solve(r.ssh_dev[:nf], form=FORM_MIXED, out=(r.ox_dev[:nf], r.oy_dev[:nf]),
                          stream=r.stream.cuda_stream)
-            r.h_ox[:nf].copy_(r.ox_dev[:nf], non_blocking=True)
-            r.h_oy[:nf].copy_(r.oy_dev[:nf], non_blocking=True)
+            f = 0
+            for q, d in zip(batch, on_dev):
+                k = q.nfields
+                if d:
+                    q.out_x = r.ox_dev[f:f + k].clone()
+                    q.out_y = r.oy_dev[f:f + k].clone()
+                else:
+                    r.h_ox[f:f + k].copy_(r.ox_dev[f:f + k], non_blocking=True)
+                    r.h_oy[f:f + k].copy_(r.oy_dev[f:f + k], non_blocking=True)
+                f += k
             r.event = torch.cuda.Event()
             r.event.record(r.stream)
 
     def _batch_done(self, r: _Resident) -> bool:
         return r.event.query()
 
-    def _results(self, r: _Resident, f: int, nfields: int):
+    def _results(self, r: _Resident, q: Request, f: int):
         r.grid.sync()
-        return r.h_ox[f:f + nfields].numpy().copy(), r.h_oy[f:f + nfields].numpy().copy()
+        if isinstance(q.ssh, self.torch.Tensor):
+            return q.out_x, q.out_y                   # written on the grid's stream before its event
+        return r.h_ox[f:f + q.nfields].numpy().copy(), r.h_oy[f:f + q.nfields].numpy().copy()
 
     # ------------------------------------------------------------------ requests
     def submit(self, req: Request) -> Request:
@@ -234,7 +269,7 @@ class Server:
             q.status = "running"
         self._launch_device(r, batch, nf)
         r.inflight = batch
-        r.last_used = self.clock()
+        r.last_used = r.launched = self.clock()
         self.grids.move_to_end(r.spec.name)
 
     def _reap(self, r: _Resident) -> None:
@@ -244,13 +279,14 @@ class Server:
         f = 0
         for q in r.inflight:
             try:
-                q.out_x, q.out_y = self._results(r, f, q.nfields)
+                q.out_x, q.out_y = self._results(r, q, f)
                 q.status = "done"
             except SalError as e:
                 q.status, q.error = "failed", e
             q.done_time = now
             f += q.nfields
             self.completed.append(q)
+        self.batches.append((r.spec.name, f, r.launched, now))
         r.inflight = None
 
     def step(self) -> int:
@@ -293,8 +329,9 @@ def poisson_arrivals(rng: np.random.Generator, rate: float, duration: float) -> 
 def run_workload(server: Server, pools: dict, weights: dict, rate: float, duration: float, seed: int = 0,
                  max_rhs: int = 16) -> list:
     """Replays Poisson arrivals in real time: each request picks a grid by
-    `weights`, 1..max_rhs fields (uniform) drawn from that grid's field pool,
-    and is submitted at its arrival time while the loop keeps batching."""
+    `weights`, 1..max_rhs fields (uniform) drawn from that grid's field pool
+    (a numpy array: host requests; a CUDA tensor: device requests), and is
+    submitted at its arrival time while the loop keeps batching."""
     rng = np.random.default_rng(seed)
     times = poisson_arrivals(rng, rate, duration)
     names = list(weights)
@@ -306,6 +343,9 @@ def run_workload(server: Server, pools: dict, weights: dict, rate: float, durati
         F = int(rng.integers(1, max_rhs + 1))
         pool = pools[name]
         idx = rng.integers(0, pool.shape[0], size=F)
+        if not isinstance(pool, np.ndarray):
+            import torch
+            idx = torch.as_tensor(idx, device=pool.device)
         plan.append((t, name, idx))
     reqs = []
     t0 = server.clock()
@@ -320,13 +360,29 @@ def run_workload(server: Server, pools: dict, weights: dict, rate: float, durati
     return reqs
 
 
-def summarize(reqs: list, cells: dict, wall: float) -> dict:
+def summarize(reqs: list, cells: dict, wall: float, batches: list | None = None) -> dict:
     done = [q for q in reqs if q.status == "done"]
     lat = np.array([q.latency for q in done]) * 1e3
     evals = sum(cells[q.grid] * q.nfields for q in done)
     single = np.array([q.latency for q in done if q.nfields == 1]) * 1e3
-    return {"requests": len(reqs), "done": len(done), "failed": sum(q.status == "failed" for q in reqs),
-            "p50_ms": float(np.percentile(lat, 50)) if len(lat) else None,
-            "p99_ms": float(np.percentile(lat, 99)) if len(lat) else None,
-            "single_field_p50_ms": float(np.percentile(single, 50)) if len(single) else None,
-            "evals_per_s": evals / wall if wall > 0 else None}
+    out = {"requests": len(reqs), "done": len(done), "failed": sum(q.status == "failed" for q in reqs),
+           "p50_ms": float(np.percentile(lat, 50)) if len(lat) else None,
+           "p99_ms": float(np.percentile(lat, 99)) if len(lat) else None,
+           "single_field_p50_ms": float(np.percentile(single, 50)) if len(single) else None,
+           "evals_per_s": evals / wall if wall > 0 else None}
+    per = {}
+    t0 = min((q.arrival for q in reqs), default=0.0)
+    for name in cells:
+        lg = np.array([q.latency for q in done if q.grid == name]) * 1e3
+        if not len(lg):
+            continue
+        d = {"requests": int(len(lg)), "p50_ms": float(np.percentile(lg, 50)), "p99_ms": float(np.percentile(lg, 99))}
+        if batches:
+            bs = [b for b in batches if b[0] == name and b[2] >= t0]
+            if bs:
+                d["batches"] = len(bs)
+                d["mean_fields_per_batch"] = float(np.mean([b[1] for b in bs]))
+                d["mean_batch_ms"] = float(np.mean([(b[3] - b[2]) * 1e3 for b in bs]))
+        per[name] = d
+    out["per_grid"] = per
+    return out

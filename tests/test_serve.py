@@ -51,9 +51,8 @@ def _fake_server(budget, max_batch=8):
             r.event -= 1
             return r.event <= 0
 
-        def _results(self, r, f, nfields):
-            q = r.inflight[[q.rid for q in r.inflight].index(r.inflight[0].rid)]
-            return np.zeros((nfields, len(r.spec.xs))), np.zeros((nfields, len(r.spec.xs)))
+        def _results(self, r, q, f):
+            return np.zeros((q.nfields, len(r.spec.xs))), np.zeros((q.nfields, len(r.spec.xs)))
 
     clock = iter(np.arange(0.0, 1e6, 1e-3))
     return FakeServer(budget, max_batch=max_batch, clock=lambda: next(clock), grid_factory=FakeGrid)
@@ -184,4 +183,11 @@ def test_served_results_equal_alone_and_in_the_mix_and_meet_accuracy():
         dx, dy = S.direct_sum(T(g.xs), T(g.ys), T(g.zs), T(g.areas * hs[f]), T(tg))
         torch.cuda.synchronize()
         assert rel_l2(q.out_x[j], q.out_y[j], dx.cpu().numpy(), dy.cpu().numpy()) <= 1e-5
+    # device-resident requests: same results as the host path
+    dreq = [(srv.submit(serve.Request(q.grid, T(grids[q.grid][1][idx]))), q) for q, idx in mix[:6]]
+    srv.run_until_idle()
+    torch.cuda.synchronize()
+    for d, q in dreq:
+        assert d.status == "done" and isinstance(d.out_x, torch.Tensor)
+        assert np.array_equal(d.out_x.cpu().numpy(), q.out_x) and np.array_equal(d.out_y.cpu().numpy(), q.out_y)
     srv.close()
