@@ -199,7 +199,7 @@ def serving_run(args, S, torch, dev):
         srv.submit(serve.Request(name, pools[name][:16]))
     srv.run_until_idle()
     t0 = time.perf_counter()
-    reqs = serve.run_workload(srv, pools, weights, args.serve_rate, args.serve_seconds, seed=7)
+    reqs = serve.run_workload(srv, pools, weights, args.serve_rate, args.serve_seconds, seed=7, keep=2)
     wall = time.perf_counter() - t0
     out = serve.summarize(reqs, sizes, wall, srv.batches)
     out.update({"rate_req_per_s": args.serve_rate, "seconds": args.serve_seconds, "max_batch_fields": 64,
@@ -208,7 +208,7 @@ def serving_run(args, S, torch, dev):
     T = lambda a: torch.tensor(a, device=dev)
     errs = []
     for name in sizes:
-        done = [q for q in reqs if q.grid == name and q.status == "done"][:2]
+        done = [q for q in reqs if q.grid == name and q.status == "done" and q.out_x is not None][:2]
         g = grids[name]
         tg = np.sort(np.random.default_rng(5).choice(g.n, min(2000, g.n), replace=False)).astype(np.int32)
         for q in done:

@@ -54,6 +54,7 @@ struct GridImpl {
     double *src_nodes = nullptr;
     double *up_partial = nullptr;
     int *err = nullptr;
+    int *h_flag = nullptr;            // pinned host copy of *err
     // batched mixed-precision form (allocated on its first solve)
     int FT = 0;                       // fields per block: 32 or 64
     int max_fields = 1;
@@ -129,6 +130,8 @@ static void grid_free(GridImpl &g) {
     g.allocs.clear();
     if (g.stream) cudaStreamDestroy(g.stream);
     g.stream = nullptr;
+    if (g.h_flag) cudaFreeHost(g.h_flag);
+    g.h_flag = nullptr;
 }
 
 static int require_device(int dev) {
@@ -226,6 +229,11 @@ extern "C" int sal_grid_create(const sal_tree *t_, const sal_grid_desc *d, sal_g
     TRY(dalloc(g, &g.up_partial, (size_t)g.nup * P));
     TRY(dalloc(g, &g.err, 1));
     CK(cudaMemset(g.err, 0, sizeof(int)));
+    if (cudaMallocHost((void **)&g.h_flag, sizeof(int)) != cudaSuccess) {
+        grid_free(g);
+        delete G;
+        return set_error(SAL_ENOMEM, "cudaMallocHost failed");
+    }
     CK(cudaDeviceSynchronize());
     // host copies no longer needed on the device side
     pl.px.clear(); pl.py.clear(); pl.pz.clear(); pl.parea.clear();
@@ -513,12 +521,15 @@ extern "C" int sal_solve(sal_grid *G, const double *ssh, int32_t nf, int64_t ld_
 }
 
 // Synchronises the grid's work on `stream` and reports a kernel time-out.
+// The flag travels on that stream (no default-stream copy), so a grid's
+// synchronisation never waits on other streams' work.
 static int finish(GridImpl &g, cudaStream_t st) {
+    CK(cudaMemcpyAsync(g.h_flag, g.err, sizeof(int), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
-    int flag = 0;
-    CK(cudaMemcpy(&flag, g.err, sizeof(int), cudaMemcpyDeviceToHost));
+    const int flag = *g.h_flag;
     if (flag) {
-        cudaMemset(g.err, 0, sizeof(int));
+        cudaMemsetAsync(g.err, 0, sizeof(int), st);
+        cudaStreamSynchronize(st);
         return set_error(SAL_ETIMEOUT, "a staging wait timed out on the device");
     }
     return SAL_OK;

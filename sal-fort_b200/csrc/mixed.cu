@@ -411,7 +411,8 @@ __global__ void finalize_mix_kernel(const int32_t *__restrict__ unit_beg, const 
 template <int KIND, int NT>
 static void launch_kind(const MixArgs &a, int ngroups, cudaStream_t st) {
     const size_t smem = sizeof(Smem);
-    cudaFuncSetAttribute(mix_kernel<KIND, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    static std::atomic<unsigned long long> done{0};
+    smem_attr_once((const void *)mix_kernel<KIND, NT>, (int)smem, done);
     mix_kernel<KIND, NT><<<ngroups, kThr, smem, st>>>(a);
 }
 

@@ -1,5 +1,6 @@
 // Launch interface of the batched mixed-precision kernels (mixed.cu).
 #pragma once
+#include <atomic>
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -7,6 +8,18 @@
 
 namespace sal {
 namespace mix {
+
+// Raises a kernel's dynamic shared memory limit once per device.  Setting a
+// function attribute while that kernel runs on another stream can stall the
+// host, so a launch path must not repeat it.
+inline void smem_attr_once(const void *fn, int bytes, std::atomic<unsigned long long> &done) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const unsigned long long bit = 1ull << (dev & 63);
+    if (done.load(std::memory_order_acquire) & bit) return;
+    cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    done.fetch_or(bit, std::memory_order_acq_rel);
+}
 
 struct MixArgs {
     const double4 *pool;      // FP64 source coordinates (points, then source proxies)

@@ -55,7 +55,7 @@ constexpr int kF = 64;                            // fields
 constexpr int kStageK = 16;                       // K columns per stage (two k-steps of 8)
 constexpr int kKStages = 3;                       // kernel-tile ring
 constexpr int kWStages = 4;                       // weight / coordinate ring
-constexpr int kMaxGroupsPerCta = 4;               // CTAs stay short (see launch_tc_leaf)
+constexpr int kMaxGroupsPerCta = 1;               // CTAs stay short (see launch_tc_leaf)
 constexpr int kTileFloats = 2048;                 // kernel tile of one k-step: 256 rows x 8, one of hi / lo
 constexpr int kWStepFloats = 1024;                // weight tile of one k-step: 128 rows x 8
 constexpr int kTmemCols = 512;
@@ -651,7 +651,8 @@ size_t tc_smem_bytes() {
 void launch_tc_leaf(const TcArgs &a, int nsm, int *err, cudaStream_t st) {
     if (a.ngroups <= 0) return;
     const size_t smem = tc_smem_bytes();
-    cudaFuncSetAttribute(tc_leaf_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    static std::atomic<unsigned long long> done{0};
+    smem_attr_once((const void *)tc_leaf_kernel, (int)smem, done);
     // every SM busy, but no CTA longer than kMaxGroupsPerCta groups, so that
     // kernels of other streams (higher-priority grids) get SMs as CTAs retire
     int grid = (a.ngroups + kMaxGroupsPerCta - 1) / kMaxGroupsPerCta;

@@ -16,7 +16,12 @@ server's device (copied device to device; results stay on the device).
 Scheduling rules:
   * a grid has at most one batch in flight (its batch buffers are its own);
   * whenever a grid is idle and has pending requests, its oldest requests are
-    packed (whole requests, at most `max_batch` fields) into the next batch;
+    packed (whole requests, at most `max_batch` fields) into the next batch --
+    at once if they fill a batch, otherwise once the oldest has waited
+    `patience` times the grid's recent batch time (a running average): a
+    batch costs about the same for 1 or 64 fields, so a grid whose batches
+    are expensive gathers more fields per batch and leaves the device to the
+    others (patience 0: launch as soon as the grid is idle);
   * grids are admitted to the device by an HBM budget: a grid whose resident
     bytes (plan + batched buffers + batch staging) do not fit evicts idle
     grids, least recently used first; a grid that alone exceeds the budget is
@@ -45,6 +50,8 @@ class Request:
     grid: str
     ssh: object                # (F, N) float64: numpy array (host) or CUDA tensor (device)
     arrival: float = 0.0
+    ready: object = None       # device requests: CUDA event after which ssh holds the fields
+                               # (None: all work queued so far on the current stream)
     rid: int = -1
     status: str = "pending"    # pending | running | done | failed | cancelled
     out_x: object = None         # same kind as ssh
@@ -52,9 +59,15 @@ class Request:
     error: Exception | None = None
     done_time: float = 0.0
 
+    nf: int = 0                # fields (kept after ssh is released)
+
+    def __post_init__(self):
+        if self.ssh is not None:
+            self.nf = self.ssh.shape[0]
+
     @property
     def nfields(self) -> int:
-        return self.ssh.shape[0]
+        return self.nf
 
     @property
     def latency(self) -> float:
@@ -92,13 +105,16 @@ class _Resident:
     event: object = None
     last_used: float = 0.0
     launched: float = 0.0
+    batch_error: Exception | None = None
+    pending_fields: int = 0
+    batch_time: float = 0.0            # running average of launch-to-done seconds
 
 
 class Server:
     """Resident grids + per-grid continuous batching on CUDA streams."""
 
     def __init__(self, hbm_budget_bytes: int, max_batch: int = 64, device: int = 0, clock=time.perf_counter,
-                 grid_factory=Grid, priorities: bool = True):
+                 grid_factory=Grid, priorities: bool = True, patience: float = 2.0):
         try:
             import torch
         except ImportError:           # the CPU test double needs no torch
@@ -115,6 +131,7 @@ class Server:
         self.completed: list[Request] = []
         self.evictions = 0
         self.priorities = priorities
+        self.patience = float(patience)
         self.batches: list[tuple] = []     # (grid, fields, launch time, done time) of finished batches
 
     # ------------------------------------------------------------------ grids
@@ -194,8 +211,18 @@ class Server:
             if not d:
                 r.h_in[f:f + q.nfields].numpy()[:] = q.ssh
             f += q.nfields
-        # device requests were written on the submitting thread's stream
-        r.stream.wait_stream(torch.cuda.current_stream(r.ssh_dev.device))
+        # device requests: wait for their fields only (a request without a
+        # ready event waits for the submitting stream); waiting on a whole
+        # low-priority stream would hand its priority to this batch
+        cur = None
+        for q, d in zip(batch, on_dev):
+            if not d:
+                continue
+            if q.ready is not None:
+                r.stream.wait_event(q.ready)
+            elif cur is None:
+                cur = torch.cuda.current_stream(r.ssh_dev.device)
+                r.stream.wait_stream(cur)
         with torch.cuda.stream(r.stream):
             f = 0
             for q, d in zip(batch, on_dev):
@@ -218,10 +245,15 @@ class Server:
             r.event.record(r.stream)
 
     def _batch_done(self, r: _Resident) -> bool:
-        return r.event.query()
+        if not r.event.query():
+            return False
+        try:
+            r.grid.sync(r.stream.cuda_stream)   # the stream is idle: only reads the grid's time-out flag
+        except SalError as e:
+            r.batch_error = e
+        return True
 
     def _results(self, r: _Resident, q: Request, f: int):
-        r.grid.sync()
         if isinstance(q.ssh, self.torch.Tensor):
             return q.out_x, q.out_y                   # written on the grid's stream before its event
         return r.h_ox[f:f + q.nfields].numpy().copy(), r.h_oy[f:f + q.nfields].numpy().copy()
@@ -238,12 +270,14 @@ class Server:
         if not req.arrival:
             req.arrival = self.clock()
         r.pending.append(req)
+        r.pending_fields += req.nfields
         return req
 
     def cancel(self, req: Request) -> bool:
         r = self.grids[req.grid]
         if req.status == "pending" and req in r.pending:
             r.pending.remove(req)
+            r.pending_fields -= req.nfields
             req.status = "cancelled"
             return True
         return False
@@ -253,6 +287,7 @@ class Server:
         batch, nf = [], 0
         while r.pending and nf + r.pending[0].nfields <= self.max_batch:
             q = r.pending.popleft()
+            r.pending_fields -= q.nfields
             batch.append(q)
             nf += q.nfields
         if not batch:
@@ -277,8 +312,11 @@ class Server:
             return
         now = self.clock()
         f = 0
+        err, r.batch_error = r.batch_error, None
         for q in r.inflight:
             try:
+                if err is not None:
+                    raise err
                 q.out_x, q.out_y = self._results(r, q, f)
                 q.status = "done"
             except SalError as e:
@@ -287,6 +325,8 @@ class Server:
             f += q.nfields
             self.completed.append(q)
         self.batches.append((r.spec.name, f, r.launched, now))
+        dt = now - r.launched
+        r.batch_time = dt if r.batch_time == 0.0 else 0.8 * r.batch_time + 0.2 * dt
         r.inflight = None
 
     def step(self) -> int:
@@ -294,11 +334,16 @@ class Server:
         batches in flight."""
         for r in self.grids.values():
             self._reap(r)
-        order = sorted((r for r in self.grids.values() if r.pending and r.inflight is None),
+        now = self.clock()
+        order = sorted((r for r in self.grids.values() if r.pending and r.inflight is None and self._ready(r, now)),
                        key=lambda r: r.pending[0].arrival)
         for r in order:
             self._launch(r)
         return sum(r.inflight is not None for r in self.grids.values())
+
+    def _ready(self, r: _Resident, now: float) -> bool:
+        return (self.patience <= 0.0 or r.pending_fields >= self.max_batch
+                or now - r.pending[0].arrival >= self.patience * r.batch_time)
 
     def busy(self) -> bool:
         return any(r.pending or r.inflight is not None for r in self.grids.values())
@@ -327,13 +372,22 @@ def poisson_arrivals(rng: np.random.Generator, rate: float, duration: float) -> 
 
 
 def run_workload(server: Server, pools: dict, weights: dict, rate: float, duration: float, seed: int = 0,
-                 max_rhs: int = 16) -> list:
+                 max_rhs: int = 16, keep: int | None = None) -> list:
     """Replays Poisson arrivals in real time: each request picks a grid by
     `weights`, 1..max_rhs fields (uniform) drawn from that grid's field pool
     (a numpy array: host requests; a CUDA tensor: device requests), and is
-    submitted at its arrival time while the loop keeps batching."""
+    submitted at its arrival time while the loop keeps batching.  With `keep`,
+    only the first `keep` finished requests of each grid hold on to their
+    fields and results; the others drop them as a client that consumed its
+    result would (holding every result of a long run would fill the device)."""
     rng = np.random.default_rng(seed)
     times = poisson_arrivals(rng, rate, duration)
+    gen = None                     # device requests are gathered on their own high-priority stream
+    for pool in pools.values():
+        if not isinstance(pool, np.ndarray):
+            import torch
+            gen = torch.cuda.Stream(device=pool.device, priority=-8)
+            break
     names = list(weights)
     p = np.array([weights[k] for k in names], dtype=float)
     p /= p.sum()
@@ -350,11 +404,26 @@ def run_workload(server: Server, pools: dict, weights: dict, rate: float, durati
     reqs = []
     t0 = server.clock()
     i = 0
+    seen, kept = len(server.completed), {}
     while i < len(plan) or server.busy():
+        if keep is not None and len(server.completed) > seen:
+            for q in server.completed[seen:]:
+                kept[q.grid] = kept.get(q.grid, 0) + 1
+                if kept[q.grid] > keep:
+                    q.ssh = q.out_x = q.out_y = None
+            seen = len(server.completed)
         now = server.clock() - t0
         while i < len(plan) and plan[i][0] <= now:
             t, name, idx = plan[i]
-            reqs.append(server.submit(Request(name, pools[name][idx], arrival=t0 + t)))
+            if gen is None:
+                reqs.append(server.submit(Request(name, pools[name][idx], arrival=t0 + t)))
+            else:
+                import torch
+                with torch.cuda.stream(gen):
+                    x = pools[name][idx]
+                    ev = torch.cuda.Event()
+                    ev.record(gen)
+                reqs.append(server.submit(Request(name, x, arrival=t0 + t, ready=ev)))
             i += 1
         server.step()
     return reqs

@@ -31,7 +31,7 @@ class FakeGrid:
         pass
 
 
-def _fake_server(budget, max_batch=8):
+def _fake_server(budget, max_batch=8, patience=0.0):
     from salgpu import serve
 
     class FakeServer(serve.Server):
@@ -55,7 +55,7 @@ def _fake_server(budget, max_batch=8):
             return np.zeros((q.nfields, len(r.spec.xs))), np.zeros((q.nfields, len(r.spec.xs)))
 
     clock = iter(np.arange(0.0, 1e6, 1e-3))
-    return FakeServer(budget, max_batch=max_batch, clock=lambda: next(clock), grid_factory=FakeGrid)
+    return FakeServer(budget, max_batch=max_batch, clock=lambda: next(clock), grid_factory=FakeGrid, patience=patience)
 
 
 def _spec(name, n, seed=0):
@@ -141,6 +141,27 @@ def test_cancel_and_malformed_requests():
     assert not srv.cancel(r1)
     srv.run_until_idle(poll_s=0)
     assert r1.status == "done" and [b[1] for b in srv.launched] == [[r1.rid]]
+
+
+def test_patience_gathers_fields_until_the_batch_fills_or_the_wait_runs_out():
+    from salgpu import serve
+    srv = _fake_server(10 ** 9, max_batch=8, patience=2.0)
+    srv.register_grid(_spec("a", 300))
+    r0 = srv.submit(serve.Request("a", np.zeros((1, 300))))
+    srv.run_until_idle(poll_s=0)                       # no batch time known yet: launches at once
+    assert [b[1] for b in srv.launched] == [[r0.rid]]
+    bt = srv.grids["a"].batch_time
+    assert bt > 0
+    r1 = srv.submit(serve.Request("a", np.zeros((2, 300))))
+    srv.step()
+    assert len(srv.launched) == 1                      # waits: 2 fields, no time has passed
+    r2 = srv.submit(serve.Request("a", np.zeros((6, 300))))
+    srv.step()                                         # 8 fields fill the batch
+    assert [b[1] for b in srv.launched][-1] == [r1.rid, r2.rid]
+    srv.run_until_idle(poll_s=0)
+    r3 = srv.submit(serve.Request("a", np.zeros((1, 300))))
+    srv.run_until_idle(poll_s=0)                       # launched once it has waited 2 batch times
+    assert r3.status == "done" and r3.done_time - r3.arrival >= 2 * bt * 0.8
 
 
 def test_poisson_arrivals_rate():
