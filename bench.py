@@ -148,8 +148,8 @@ def cpu_baseline(args, g, h, sample_seconds):
 
 def workload_name(args, n):
     form = {"ref": "plain FP64 (reference operation order)", "accurate": "FP64 accurate form",
-            "mixed": "batched mixed precision: FP32 kernel tiles, TF32 3-pass tensor-core contractions, "
-                     "FP64 self pairs"}[args.form]
+            "mixed": "batched mixed precision: FP32 kernel tiles, TF32 hi/lo tensor-core contractions "
+                     "(tcgen05 leaf pass), FP64 self pairs"}[args.form]
     return (f"{args.config}: {n} cells x {args.fields} SSH fields, dual tree traversal (code.f90 fast_sum), "
             f"d={args.degree}, theta={args.theta}, leaf<{args.thresh}; {form}")
 
@@ -352,12 +352,13 @@ def main():
         peak = bf16 / 2.0          # dense TF32 = half the bf16 rate
         leaf_flops = 4.0 * F * (st["pairs_pp"] + st["pairs_pc"] + 3.0 * st["macs_down"])
         achieved = leaf_flops / (leaf_ms * 1e-3) / 1e12
-        roof = {"bound": "tensor", "kernel": "mix_kernel<leaf> (PP+PC kernel tiles, DOWN interpolation)",
+        roof = {"bound": "tensor", "kernel": "tc_leaf_kernel (tcgen05 TF32 hi/lo, M=128 field parts x N=256 target "
+                          "components; PP+PC kernel tiles, DOWN interpolation) + split_store_kernel",
                 "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
                 "peak_source": ("TF32 dense = bf16_tflops/2 of measured" if "bf16_tflops" in peaks else
                                 "TF32 dense = 1.59 PFLOP/s bf16 fallback / 2"),
-                "flops_counted": "algorithmic 4*F per pair (2 components x FMA x F fields); the TF32 3-pass "
-                                 "split executes 3x these on the tensor cores",
+                "flops_counted": "algorithmic 4*F per pair (2 components x FMA x F fields); the hi/lo split "
+                                 "executes 4x these on the tensor cores (W_hi,W_lo x T_hi,T_lo), plus padding",
                 "traffic": None, "leaf_ms": leaf_ms, "proxy_ms": proxy_ms, "prep_upward_ms": up_ms}
     else:
         peak64 = S.fma_peak(64)
@@ -397,7 +398,8 @@ def main():
             "e2e": {"value": e2e_val, "unit": "evals/s", "h2d_bytes_per_step": 8 * g.n * F,
                     "d2h_bytes_per_step": 16 * g.n * F, "api": "sal_solve_host (pinned host buffers)"},
             "clocks": clocks,
-            "gpu_launches": 6 * args.steps * (((F + 63) // 64) if F > 32 else 1) if form == S.FORM_MIXED else 6 * args.steps,
+            # batched form: prep, upward, finalize, proxy, finalize, split store, leaf per 64-field block
+            "gpu_launches": 7 * args.steps * (((F + 63) // 64) if F > 32 else 1) if form == S.FORM_MIXED else 6 * args.steps,
         }
         if cb:
             line["cpu_baseline"] = cb
