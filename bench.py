@@ -359,7 +359,11 @@ def main():
                                 "TF32 dense = 1.59 PFLOP/s bf16 fallback / 2"),
                 "flops_counted": "algorithmic 4*F per pair (2 components x FMA x F fields); the hi/lo split "
                                  "executes 4x these on the tensor cores (W_hi,W_lo x T_hi,T_lo), plus padding",
-                "traffic": None, "leaf_ms": leaf_ms, "proxy_ms": proxy_ms, "prep_upward_ms": up_ms}
+                # ncu dram__bytes_read.sum + dram__bytes_write.sum of one tc_leaf_kernel launch on the
+                # 655,362-cell, 64-field case (3.53 + 2.62 GB), scaled by the cell count
+                "traffic": 6.156e9 * g.n / 655362 if F == 64 else None,
+                "traffic_source": "ncu capture on 655,362 cells x 64 fields, scaled by cells",
+                "leaf_ms": leaf_ms, "proxy_ms": proxy_ms, "prep_upward_ms": up_ms}
     else:
         peak64 = S.fma_peak(64)
         leaf_flops = FLOPS_PER_PAIR * (st["pairs_pp"] + st["pairs_pc"]) + 2 * FLOPS_PER_MAC * st["macs_down"]
