@@ -367,8 +367,12 @@ __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(TcArgs a, int *err
                 self_e = (float)sk.x;
                 self_n = (float)sk.y;
             }
+            // item records are read one item ahead, so their latency hides
+            // behind the current item's stages
+            TcItem nxt = a.items[G.ib];
             for (int k = 0; k < ni; ++k) {
-                const TcItem it = a.items[G.ib + k];
+                const TcItem it = nxt;
+                if (k + 1 < ni) nxt = a.items[G.ib + k + 1];
                 const int kind = it.kind & 3;
                 const int nst = (it.cnt + kStageK - 1) / kStageK;
                 if (kind == 2 && it.off != cur_slot) {
@@ -469,8 +473,10 @@ __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(TcArgs a, int *err
         bool chain_open = false;
         for (int gi = blockIdx.x; gi < a.ngroups; gi += gridDim.x) {
             const MixGroup G = a.groups[gi];
+            TcItem nxt = G.ib < G.ie ? a.items[G.ib] : TcItem{};
             for (int k = G.ib; k < G.ie; ++k) {
-                const TcItem it = a.items[k];
+                const TcItem it = nxt;
+                if (k + 1 < G.ie) nxt = a.items[k + 1];
                 const int nst = (it.cnt + kStageK - 1) / kStageK;
                 for (int j = 0; j < nst; ++j, ++st) {
                     const uint32_t slot = st % kKStages, jb = st % kWStages;
@@ -514,8 +520,10 @@ __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(TcArgs a, int *err
         // ============================================================ loads
         for (int gi = blockIdx.x; gi < a.ngroups; gi += gridDim.x) {
             const MixGroup G = a.groups[gi];
+            TcItem nxt = G.ib < G.ie ? a.items[G.ib] : TcItem{};
             for (int k = G.ib; k < G.ie; ++k) {
-                const TcItem it = a.items[k];
+                const TcItem it = nxt;
+                if (k + 1 < G.ie) nxt = a.items[k + 1];
                 const int nst = (it.cnt + kStageK - 1) / kStageK;
                 for (int j = 0; j < nst; ++j, ++st) {
                     const uint32_t jb = st % kWStages, ub = st / kWStages;
