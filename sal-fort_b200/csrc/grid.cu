@@ -62,10 +62,13 @@ struct GridImpl {
     MixGroup *mix_leaf_groups = nullptr, *mix_proxy_groups = nullptr, *mix_up_groups = nullptr;
     MixGroup *tc_leaf_groups = nullptr;
     TcItem *tc_items = nullptr;
+    MixGroup *tc_proxy_groups = nullptr;
+    TcItem *tc_proxy_items = nullptr;
     int32_t *bsrc = nullptr;
     float *bstore = nullptr;          // split weight store of the tcgen05 leaf pass
     float4 *sloc = nullptr;
     float *sxyz = nullptr;
+    int32_t *iperm = nullptr;         // caller index -> pool position
     double2 *selfk = nullptr;
     int nsm = 0;
     Item *mix_leaf_items = nullptr, *mix_proxy_items = nullptr;
@@ -359,6 +362,11 @@ static int ensure_mixed(GridImpl &g, int FT) {
     if (!rc) rc = dalloc(g, &g.phiF, (size_t)g.ntgt * 3 * P * FT);
     if (!rc) rc = dalloc(g, &g.mix_up_partial, (size_t)g.nup * P * FT);
     if (!rc) rc = dalloc(g, &g.mix_proxy_partial, (size_t)g.nproxy_units * 3 * P * FT);
+    if (!rc) {
+        std::vector<int32_t> ip(n);
+        for (size_t p = 0; p < n; ++p) ip[(size_t)pl.perm[p]] = (int32_t)p;
+        rc = dupload(g, &g.iperm, ip.data(), ip.size());
+    }
     if (!rc) rc = dupload(g, &g.mix_leaf_groups, pl.mix_leaf_groups.data(), pl.mix_leaf_groups.size());
     if (!rc) rc = dupload(g, &g.mix_leaf_items, pl.mix_leaf_items.data(), pl.mix_leaf_items.size());
     if (!rc) rc = dupload(g, &g.mix_proxy_groups, pl.mix_proxy_groups.data(), pl.mix_proxy_groups.size());
@@ -369,6 +377,8 @@ static int ensure_mixed(GridImpl &g, int FT) {
         // coordinates and the per-point self pairs
         rc = dupload(g, &g.tc_leaf_groups, pl.tc_leaf_groups.data(), pl.tc_leaf_groups.size());
         if (!rc) rc = dupload(g, &g.tc_items, pl.tc_items.data(), pl.tc_items.size());
+        if (!rc) rc = dupload(g, &g.tc_proxy_groups, pl.tc_proxy_groups.data(), pl.tc_proxy_groups.size());
+        if (!rc) rc = dupload(g, &g.tc_proxy_items, pl.tc_proxy_items.data(), pl.tc_proxy_items.size());
         if (!rc) rc = dupload(g, &g.bsrc, pl.bsrc.data(), pl.bsrc.size());
         if (!rc) rc = dalloc(g, &g.bstore, pl.bsrc.size() * 2 * (size_t)FT);
         if (!rc) rc = dalloc(g, &g.sloc, n + (size_t)g.nsrc * P);
@@ -413,7 +423,7 @@ static void solve_mixed_block(GridImpl &g, const double *ssh, int64_t ld_ssh, in
     const Plan &pl = g.plan;
     const int n = pl.n, P = pl.P, FT = g.FT;
     if (g.timing) cudaEventRecord(g.ev[0], st);
-    mix::launch_prep_mix(g.area, ssh, ld_ssh, g.perm, n, f0, nf, FT, g.wF, st);
+    mix::launch_prep_mix(g.area, ssh, ld_ssh, g.iperm, n, f0, nf, FT, g.wF, st);
     mix::MixArgs a{};
     a.pool = g.pool;
     a.wF = g.wF;
@@ -439,7 +449,23 @@ static void solve_mixed_block(GridImpl &g, const double *ssh, int64_t ld_ssh, in
         mix::launch_finalize_mix(g.up_unit_beg, g.mix_up_partial, g.nsrc, P, FT, g.wF + (size_t)n * FT, st);
     }
     if (g.timing) cudaEventRecord(g.ev[1], st);
-    if (!pl.mix_proxy_groups.empty()) {
+    // 64-field blocks: the source rows of the split weight store (points and
+    // proxy weights are final now), then the proxy pass on tcgen05
+    if (g.bstore) mix::launch_split_store(g.bsrc, 0, pl.tc_src_ksteps, g.wF, g.phiF, g.bstore, st);
+    if (g.bstore && !pl.tc_proxy_groups.empty()) {
+        mix::TcArgs p{};
+        p.groups = g.tc_proxy_groups;
+        p.ngroups = (int)pl.tc_proxy_groups.size();
+        p.items = g.tc_proxy_items;
+        p.sxyz = g.sxyz;
+        p.bstore = g.bstore;
+        p.tgt = g.tgt_proxy;
+        p.d = pl.d;
+        p.P = P;
+        p.partial = g.mix_proxy_partial;
+        mix::launch_tc_proxy(p, g.nsm, g.err, st);
+        mix::launch_finalize_mix(g.proxy_unit_beg, g.mix_proxy_partial, g.ntgt, 3 * P, FT, g.phiF, st);
+    } else if (!pl.mix_proxy_groups.empty()) {
         mix::MixArgs q = a;
         q.groups = g.mix_proxy_groups;
         q.items = g.mix_proxy_items;
@@ -453,8 +479,9 @@ static void solve_mixed_block(GridImpl &g, const double *ssh, int64_t ld_ssh, in
     a.tgt = g.pool;
     a.tgt_nodes = g.tgt_nodes;
     if (g.bstore) {
-        // 64-field blocks: split weight store, then the tcgen05 leaf pass
-        mix::launch_split_store(g.bsrc, (int64_t)pl.bsrc.size(), g.wF, g.phiF, g.bstore, st);
+        // 64-field blocks: the potential rows of the split weight store, then
+        // the tcgen05 leaf pass
+        mix::launch_split_store(g.bsrc, pl.tc_src_ksteps, (int64_t)pl.bsrc.size() / 8, g.wF, g.phiF, g.bstore, st);
         mix::TcArgs t{};
         t.groups = g.tc_leaf_groups;
         t.ngroups = (int)pl.tc_leaf_groups.size();

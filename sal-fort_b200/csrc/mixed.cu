@@ -377,20 +377,31 @@ __global__ void __launch_bounds__(kThr) mix_kernel(MixArgs a) {
     }
 }
 
-// ------------------------------------------------------------------ per-field source weights
-// kCons * area * ssh: the kernel's constant factor travels with the weights,
-// so every contraction (PP, PC, upward, CP/CC and DOWN) produces scaled results.
+// Per-field FP32 weights of the points in pool order: wF[pos][f] =
+// kCons * area[pos] * ssh[f0 + f][caller index], zero for fields past nf.
+// One block transposes a tile of 32 consecutive caller indices x FT fields
+// through shared memory, so the reads of ssh (caller order, field-major) and
+// the writes of wF (pool order, field-minor) are both whole rows.
 __global__ void prep_mix_kernel(const double *__restrict__ area, const double *__restrict__ ssh, int64_t ld,
-                                const int32_t *__restrict__ perm, int n, int f0, int nf, int FT,
+                                const int32_t *__restrict__ iperm, int n, int f0, int nf, int FT,
                                 float *__restrict__ wF) {
-    const int pos = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
-    if (pos >= n) return;
-    const int lane = threadIdx.x & 31;
-    const int idx = perm[pos];
-    const double ar = area[pos];
-    for (int f = lane; f < FT; f += 32) {
+    __shared__ float tile[32][64 + 1];
+    __shared__ int pos_s[32];
+    const int idx0 = blockIdx.x * 32, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int idx = idx0 + lane;
+    const bool live = idx < n;
+    const int pos = live ? iperm[idx] : 0;
+    const double scale = live ? dev::kCons * area[pos] : 0.0;
+    if (warp == 0) pos_s[lane] = live ? pos : -1;
+    for (int f = warp; f < FT; f += blockDim.x >> 5) {
         const int ff = f0 + f;
-        wF[(size_t)pos * FT + f] = ff < nf ? (float)(dev::kCons * ar * ssh[(size_t)ff * ld + idx]) : 0.f;
+        tile[lane][f] = (live && ff < nf) ? (float)(scale * ssh[(size_t)ff * ld + idx]) : 0.f;
+    }
+    __syncthreads();
+    for (int r = warp; r < 32; r += blockDim.x >> 5) {
+        const int p = pos_s[r];
+        if (p < 0) continue;
+        for (int f = lane; f < FT; f += 32) wF[(size_t)p * FT + f] = tile[r][f];
     }
 }
 
@@ -429,10 +440,10 @@ void launch_mix(int kind, int FT, const MixArgs &a, int ngroups, cudaStream_t st
     }
 }
 
-void launch_prep_mix(const double *area, const double *ssh, int64_t ld, const int32_t *perm, int n, int f0, int nf,
+void launch_prep_mix(const double *area, const double *ssh, int64_t ld, const int32_t *iperm, int n, int f0, int nf,
                      int FT, float *wF, cudaStream_t st) {
     if (n <= 0) return;
-    prep_mix_kernel<<<(n + 7) / 8, 256, 0, st>>>(area, ssh, ld, perm, n, f0, nf, FT, wF);
+    prep_mix_kernel<<<(n + 31) / 32, 256, 0, st>>>(area, ssh, ld, iperm, n, f0, nf, FT, wF);
 }
 
 void launch_finalize_mix(const int32_t *unit_beg, const float *partial, int nslots, int rows_per_slot, int FT,

@@ -42,7 +42,7 @@ struct MixArgs {
 };
 
 void launch_mix(int kind, int FT, const MixArgs &a, int ngroups, cudaStream_t st);
-void launch_prep_mix(const double *area, const double *ssh, int64_t ld, const int32_t *perm, int n, int f0, int nf,
+void launch_prep_mix(const double *area, const double *ssh, int64_t ld, const int32_t *iperm, int n, int f0, int nf,
                      int FT, float *wF, cudaStream_t st);
 void launch_finalize_mix(const int32_t *unit_beg, const float *partial, int nslots, int rows_per_slot, int FT,
                          float *dst, cudaStream_t st);
@@ -64,11 +64,13 @@ struct TcArgs {
     double *out_x, *out_y;    // caller's outputs (column f at + f*ld_out)
     int64_t ld_out;
     int f0, nf;
+    float *partial;           // proxy pass: per-unit rows (P x 3 components x 64 fields)
 };
 void launch_tc_leaf(const TcArgs &a, int nsm, int *err, cudaStream_t st);
+void launch_tc_proxy(const TcArgs &a, int nsm, int *err, cudaStream_t st);
 size_t tc_smem_bytes();
-void launch_split_store(const int32_t *bsrc, int64_t nrows, const float *wF, const float *phiF, float *bstore,
-                        cudaStream_t st);
+void launch_split_store(const int32_t *bsrc, int64_t k0, int64_t k1, const float *wF, const float *phiF,
+                        float *bstore, cudaStream_t st);
 void launch_source_local(const double4 *pool, const int2 *ranges, const double4 *centres, int nranges, float4 *sloc,
                          cudaStream_t st);
 void launch_self_pair(const double4 *pool, int n, double2 *selfk, cudaStream_t st);

@@ -351,6 +351,8 @@ bool plan_build(const Tree &t, int d, int mode, const int32_t *list, int64_t nli
     // range padded with zero rows to a multiple of 8 so that each item starts
     // on a k-step boundary and its padding columns meet zero weights.
     pl->tc_items.clear();
+    pl->tc_proxy_items.clear();
+    pl->tc_proxy_groups.clear();
     pl->bsrc.clear();
     pl->sloc_ranges.clear();
     pl->sloc_centres.clear();
@@ -383,13 +385,11 @@ bool plan_build(const Tree &t, int d, int mode, const int32_t *list, int64_t nli
             for (int r = 0; r < P; ++r) pl->bsrc[src_b0 + s * P8 + r] = (int32_t)(n + (int64_t)s * P + r);
         for (int32_t s = 0; s < ntgt; ++s)
             for (int r = 0; r < 3 * P; ++r) pl->bsrc[phi_b0 + s * P38 + r] = (int32_t)(-2 - ((int64_t)s * 3 * P + r));
-        std::vector<int32_t> gord(pl->leaf_groups.size());
-        std::iota(gord.begin(), gord.end(), 0);
-        std::sort(gord.begin(), gord.end(), [&](int a, int b) { return pl->leaf_groups[a].tgt < pl->leaf_groups[b].tgt; });
-        for (int32_t gi : gord) {
-            const Group &g = pl->leaf_groups[gi];
-            const int kt = leaves[g.out];
-            const int32_t ib = (int32_t)pl->tc_items.size();
+        // One work list (items [ib, ie) of `src`) as tcgen05 items relative to
+        // the centre of target panel kt, with the accumulator-chain flags.
+        auto convert = [&](const std::vector<Item> &src, int32_t ib0, int32_t ie0, int kt,
+                           std::vector<TcItem> &dst) -> bool {
+            const int32_t ib = (int32_t)dst.size();
             auto push = [&](int kind, int64_t off, int64_t total, int64_t base, int ks) {
                 TcItem r{};
                 r.kind = kind;
@@ -403,22 +403,21 @@ bool plan_build(const Tree &t, int d, int mode, const int32_t *list, int64_t nli
                     r.kb = (int32_t)((base + b) / 8);
                     r.off = (int32_t)(kind == 2 ? off : off + b);
                     r.row0 = kind == 2 ? (int32_t)b : 0;
-                    pl->tc_items.push_back(r);
+                    dst.push_back(r);
                 }
             };
-            for (int32_t i = g.ib; i < g.ie; ++i) {
-                const Item &it = pl->leaf_items[i];
+            for (int32_t i = ib0; i < ie0; ++i) {
+                const Item &it = src[i];
                 if (it.kind == 0) {
-                    // a PP source panel's range, re-joined across the staging
-                    // splits and cut at leaf boundaries
+                    // a point source panel's range, re-joined across the
+                    // staging splits and cut at leaf boundaries
                     int64_t b = it.off, e = (int64_t)it.off + it.cnt;
-                    while (i + 1 < g.ie && pl->leaf_items[i + 1].kind == 0 && pl->leaf_items[i + 1].off == e)
-                        e += pl->leaf_items[++i].cnt;
+                    while (i + 1 < ie0 && src[i + 1].kind == 0 && src[i + 1].off == e) e += src[++i].cnt;
                     while (b < e) {
                         const int32_t l = leaf_of_pos[b];
                         const Panel &q = t.p[leaves[l]];
                         const int64_t le = std::min<int64_t>(e, q.end);
-                        if ((b - q.begin) % 8 != 0) { *err = "internal: PP range starts inside a leaf"; return false; }
+                        if ((b - q.begin) % 8 != 0) { *err = "internal: point range starts inside a leaf"; return false; }
                         push(0, b, le - b, leaf_b[l] + (b - q.begin), leaves[l]);
                         b = le;
                     }
@@ -429,19 +428,44 @@ bool plan_build(const Tree &t, int d, int mode, const int32_t *list, int64_t nli
                     push(2, it.off, 3 * P, phi_b0 + (int64_t)it.off * P38, -1);
                 }
             }
-            const int32_t ie = (int32_t)pl->tc_items.size();
+            const int32_t ie = (int32_t)dst.size();
             // accumulator chains: end one after the item that brings it to
-            // kTcChainKSteps k-steps, and always after the group's last item
+            // kTcChainKSteps k-steps, and always after the list's last item
             for (int32_t i = ib, chain = 0; i < ie; ++i) {
-                TcItem &r = pl->tc_items[i];
+                TcItem &r = dst[i];
                 chain += (r.cnt + 7) / 8;
                 if (chain >= kTcChainKSteps || i == ie - 1) { r.kind |= kTcFlush; chain = 0; }
             }
+            return true;
+        };
+        std::vector<int32_t> gord(pl->leaf_groups.size());
+        std::iota(gord.begin(), gord.end(), 0);
+        std::sort(gord.begin(), gord.end(), [&](int a, int b) { return pl->leaf_groups[a].tgt < pl->leaf_groups[b].tgt; });
+        for (int32_t gi : gord) {
+            const Group &g = pl->leaf_groups[gi];
+            const int kt = leaves[g.out];
+            const int32_t ib = (int32_t)pl->tc_items.size();
+            if (!convert(pl->leaf_items, g.ib, g.ie, kt, pl->tc_items)) return false;
+            const int32_t ie = (int32_t)pl->tc_items.size();
             for (int32_t r = 0; r < g.nt; r += kTcRows) {
                 MixGroup m{};
                 m.tgt = g.tgt + r; m.nt = std::min(kTcRows, g.nt - r); m.ib = ib; m.ie = ie; m.out = g.out;
                 m.cx = t.cx[kt]; m.cy = t.cy[kt]; m.cz = t.cz[kt];
                 pl->tc_leaf_groups.push_back(m);
+            }
+        }
+        // proxy pass: per unit of a target slot, rows of at most kTcProxyRows
+        // proxies (three Cartesian components each fill the MMA's N = 256)
+        for (const Group &g : pl->proxy_groups) {
+            const int kt = pl->tgt_slot_panel[g.tgt];
+            const int32_t ib = (int32_t)pl->tc_proxy_items.size();
+            if (!convert(pl->proxy_items, g.ib, g.ie, kt, pl->tc_proxy_items)) return false;
+            const int32_t ie = (int32_t)pl->tc_proxy_items.size();
+            for (int32_t r = 0; r < P; r += kTcProxyRows) {
+                MixGroup m{};
+                m.tgt = g.tgt; m.nt = std::min(kTcProxyRows, P - r); m.ib = ib; m.ie = ie; m.out = g.out; m.row0 = r;
+                m.cx = t.cx[kt]; m.cy = t.cy[kt]; m.cz = t.cz[kt];
+                pl->tc_proxy_groups.push_back(m);
             }
         }
     }

@@ -128,6 +128,10 @@ struct Plan {
     // slot and target slot starts on a multiple of 8 rows).
     std::vector<MixGroup> tc_leaf_groups;
     std::vector<TcItem> tc_items;
+    // tcgen05 proxy pass: per proxy unit, row chunks of at most kTcProxyRows
+    // target proxies (row0 = first proxy, out = unit), and their items
+    std::vector<MixGroup> tc_proxy_groups;
+    std::vector<TcItem> tc_proxy_items;
     std::vector<int32_t> bsrc;
     int64_t tc_src_ksteps = 0;                    // k-steps of the store holding sources (points, proxies)
     // pool row ranges (begin, end) of every leaf and every source slot's
@@ -149,6 +153,7 @@ constexpr int kMixStage = 64;    // sources (or DOWN rows) staged per batched it
 constexpr int kMixRows = 64;     // targets per batched CTA
 constexpr int kTcRows = 128;     // targets per tcgen05 leaf group (the MMA's M)
 constexpr int kTcChunk = 64;     // sources (or DOWN rows) per tcgen05 item
+constexpr int kTcProxyRows = 85;   // target proxies per tcgen05 proxy group: 3 x 85 <= 256
 constexpr int kTcChainKSteps = 32;  // k-steps (8 sources) an accumulator chain reaches before it is folded
 constexpr int kMaxDegree = 14;   // a DOWN record (4(d+1)^2 + 2(d+1) doubles) fits one 8 KB stage
 

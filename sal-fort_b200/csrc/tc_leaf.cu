@@ -1,4 +1,10 @@
-// Leaf pass of the batched form on the 5th-generation tensor cores (tcgen05).
+// Leaf pass (MODE 0) and proxy pass (MODE 1) of the batched form on the
+// 5th-generation tensor cores (tcgen05).  The proxy pass is the same machine
+// with the Chebyshev proxies of a target slot as targets (at most 85 per
+// group), three Cartesian components val (s - x) instead of the projected
+// east / north ones (3 x 85 columns fill N = 256), no self pairs, no DOWN
+// items, and the group's end written to its unit's partial rows.  The leaf
+// pass is described below.
 //
 // One CTA per SM at a time, each walking a few leaf groups of up to 128
 // targets in pool order with a stride of the grid size.  A group's work is a list of
@@ -201,8 +207,9 @@ __host__ __device__ constexpr int wrow(int f, int part) { return 32 * (f >> 4) +
 // end: running sum + chain to the caller's outputs for its nt targets.
 // Tensor memory loads are double-buffered and each 16-column chunk reads its
 // 8 running-sum entries before it writes any, so the chunk's latencies overlap.
+template <int MODE>
 __device__ __forceinline__ void fold_chunk(const float (&x)[16], int c0, float *run, int f, int odd, bool end,
-                                           bool first, int nt, int idk, double *out, int64_t ld_out, bool wr) {
+                                           bool first, int nt, int idk, double *out, bool wr, float *part) {
     float v[8], rs[8];
     float *rp[8];
 #pragma unroll
@@ -223,29 +230,43 @@ __device__ __forceinline__ void fold_chunk(const float (&x)[16], int c0, float *
     if (!end) {
 #pragma unroll
         for (int m = 0; m < 8; ++m) *rp[m] = v[m];
-    } else {
+    } else if (MODE == 0) {
 #pragma unroll
         for (int m = 0; m < 8; ++m) {
             const int t = (c0 & 127) + 2 * m + odd;
             const int ti = __shfl_sync(0xffffffffu, idk, t & 31);
             if (wr && t < nt) out[ti] = (double)v[m];
         }
+    } else {
+        // proxy rows: column j = 85c + r is component c of proxy r; the unit's
+        // partial holds (proxy, component) rows of 64 fields
+#pragma unroll
+        for (int m = 0; m < 8; ++m) {
+            const int j = c0 + 2 * m + odd, c = j / kTcProxyRows, r = j - c * kTcProxyRows;
+            if (wr && c < 3 && r < nt) part[((size_t)r * 3 + c) * kF + f] = v[m];
+        }
     }
 }
 
+// MODE 0 (leaf): columns 128c + t are component c (east, north) of target t,
+// ends go to the caller's outputs.  MODE 1 (proxy): columns 85c + r are
+// Cartesian component c of proxy r, ends go to the unit's partial rows `part`.
+template <int MODE>
 __device__ __noinline__ void fold_chain(uint32_t td, float *run, int q, int lane, bool end, bool first, int tgt,
                                         int nt, const int32_t *__restrict__ perm, double *out_x, double *out_y,
-                                        int64_t ld_out, int f0, int nf, bool skip) {
+                                        int64_t ld_out, int f0, int nf, bool skip, float *part) {
     const int f = 16 * q + (lane & 15), odd = lane >> 4;
     int idx[4] = {0, 0, 0, 0};   // caller index of target slot 32k + lane
-    if (end)
+    if (MODE == 0 && end)
 #pragma unroll
         for (int k = 0; k < 4; ++k) idx[k] = 32 * k + lane < nt ? perm[tgt + 32 * k + lane] : 0;
-    const bool wr = end && f0 + f < nf && !skip;
-    double *ox = out_x + (size_t)(f0 + f) * ld_out, *oy = out_y + (size_t)(f0 + f) * ld_out;
-    // chunks of 16 columns: component ch = c / 128, target slots c % 128 ..+15;
-    // at a group's end only the chunks that hold targets
-    const int per = end ? (nt + 15) / 16 : 8;
+    const bool wr = end && (MODE == 1 || f0 + f < nf) && !skip;
+    double *ox = MODE == 0 ? out_x + (size_t)(f0 + f) * ld_out : nullptr;
+    double *oy = MODE == 0 ? out_y + (size_t)(f0 + f) * ld_out : nullptr;
+    // chunks of 16 columns: leaf component ch = c / 128, target slots
+    // c % 128 ..+15 (at a group's end only the chunks that hold targets);
+    // proxy: all 16 chunks
+    const int per = (MODE == 0 && end) ? (nt + 15) / 16 : 8;
     const int nchunk = 2 * per;
     auto col = [&](int i) { return (i / per) * 128 + (i % per) * 16; };
     float xa[16], xb[16];
@@ -257,18 +278,19 @@ __device__ __noinline__ void fold_chain(uint32_t td, float *run, int q, int lane
         {
             const int c = col(i), ik = (c & 127) >> 5;
             const int idk = ik == 0 ? idx[0] : ik == 1 ? idx[1] : ik == 2 ? idx[2] : idx[3];
-            fold_chunk(xa, c, run, f, odd, end, first, nt, idk, c < 128 ? ox : oy, ld_out, wr);
+            fold_chunk<MODE>(xa, c, run, f, odd, end, first, nt, idk, c < 128 ? ox : oy, wr, part);
         }
         if (i + 1 < nchunk) {
             tmem_wait_ld();
             if (i + 2 < nchunk) tmem_ld16(td + col(i + 2), xa);
             const int c = col(i + 1), ik = (c & 127) >> 5;
             const int idk = ik == 0 ? idx[0] : ik == 1 ? idx[1] : ik == 2 ? idx[2] : idx[3];
-            fold_chunk(xb, c, run, f, odd, end, first, nt, idk, c < 128 ? ox : oy, ld_out, wr);
+            fold_chunk<MODE>(xb, c, run, f, odd, end, first, nt, idk, c < 128 ? ox : oy, wr, part);
         }
     }
 }
 
+template <int MODE>
 __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(TcArgs a, int *err) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     TcSmem &sm = *reinterpret_cast<TcSmem *>(smem_raw);
@@ -315,8 +337,12 @@ __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(TcArgs a, int *err
     if (warp < kProdWarps) {
         // ============================================================ producers
         const int row = tid & (kTcRows - 1), ks = tid >> 7;      // generation: target row, k-step of the stage
-        // canonical offsets (floats) of this thread's east / north rows in a kernel tile
-        const int oe = canon(row, 0) >> 2, on = canon(kTcRows + row, 0) >> 2;
+        // canonical offsets (floats) of this thread's rows in a kernel tile:
+        // leaf east / north at rows t, 128 + t; proxy x / y / z at 85c + r
+        const int oe = canon(MODE == 0 ? row : row, 0) >> 2;
+        const int on = canon(MODE == 0 ? kTcRows + row : kTcProxyRows + row, 0) >> 2;
+        const int oz = canon(MODE == 0 ? 0 : 2 * kTcProxyRows + row, 0) >> 2;
+        const bool row_in_tile = MODE == 0 || row < kTcProxyRows;
         // wait for a free kernel-tile slot
         auto wait_slot = [&](uint32_t s) {
             if (s >= (uint32_t)kKStages)
@@ -331,11 +357,12 @@ __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(TcArgs a, int *err
             // north unit vectors (zero at the poles, as the reference's guard)
             float tl0 = 0.f, tl1 = 0.f, tl2 = 0.f, el0 = 0.f, el1 = 0.f, ep0 = 0.f, ep1 = 0.f, ep2 = 0.f;
             if (rvalid) {
-                const double4 c = a.tgt[G.tgt + row];
+                // leaf: the pool point; proxy: proxy row0 + row of target slot G.tgt
+                const double4 c = MODE == 0 ? a.tgt[G.tgt + row] : a.tgt[(size_t)G.tgt * P + G.row0 + row];
                 tl0 = (float)(c.x - G.cx);
                 tl1 = (float)(c.y - G.cy);
                 tl2 = (float)(c.z - G.cz);
-                if ((fabs(c.z - 1.0) > 1e-15) && (fabs(c.z + 1.0) > 1e-15)) {
+                if (MODE == 0 && (fabs(c.z - 1.0) > 1e-15) && (fabs(c.z + 1.0) > 1e-15)) {
                     const double omz = 1.0 - c.z * c.z, inv = 1.0 / sqrt(omz);
                     el0 = (float)(-c.y * inv);
                     el1 = (float)(c.x * inv);
@@ -346,7 +373,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(TcArgs a, int *err
             }
             if (ni == 0) {
                 // no sources: the self pair alone
-                if (rvalid && ks == 0 && !*abort) {
+                if (MODE == 0 && rvalid && ks == 0 && !*abort) {
                     const int pos = G.tgt + row, idx = a.perm[pos];
                     const double2 sk = a.selfk[pos];
                     for (int f = 0; f < kF && a.f0 + f < a.nf; ++f) {
@@ -362,7 +389,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(TcArgs a, int *err
             // the self pair (FP64 value / kernel constant, the weight carries the constant)
             const int my_pos = G.tgt + row;
             float self_e = 0.f, self_n = 0.f;
-            if (rvalid) {
+            if (MODE == 0 && rvalid) {
                 const double2 sk = a.selfk[my_pos];
                 self_e = (float)sk.x;
                 self_n = (float)sk.y;
@@ -375,7 +402,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(TcArgs a, int *err
                 if (k + 1 < ni) nxt = a.items[G.ib + k + 1];
                 const int kind = it.kind & 3;
                 const int nst = (it.cnt + kStageK - 1) / kStageK;
-                if (kind == 2 && it.off != cur_slot) {
+                if (MODE == 0 && kind == 2 && it.off != cur_slot) {
                     // BLI bases of every target row in the new slot: thread
                     // (row, 0) the xi basis, thread (row, 1) the eta basis
                     cur_slot = it.off;
@@ -393,8 +420,8 @@ __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(TcArgs a, int *err
                     wait_slot(st);
                     const uint32_t slot = st % kKStages;
                     if (active) {
-                        float ve[8], vn[8];
-                        if (kind == 2) {
+                        float ve[8], vn[8], vz[8];
+                        if (MODE == 0 && kind == 2) {
                             // DOWN: BLI basis of the target x its unit vector's
                             // component of the Cartesian row
                             const int *km0 = sm.kmap + it.row0 + kStageK * j + 8 * ks;
@@ -427,17 +454,28 @@ __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(TcArgs a, int *err
                                 const float2 u = make_float2(rcp_approx(w.x), rcp_approx(w.y));
                                 const float2 inner = __ffma2_rn(f2(kC1F), r, __ffma2_rn(f2(kTwoC2F), u, f2(-kTwoC2F)));
                                 const float2 v = __fmul2_rn(inner, __fmul2_rn(r, r));
-                                const float2 pe = __ffma2_rn(el1v, dy, __fmul2_rn(el0v, dx));
-                                const float2 pn = __ffma2_rn(ep2v, dz, __ffma2_rn(ep1v, dy, __fmul2_rn(ep0v, dx)));
-                                const float2 e2 = __fmul2_rn(v, pe), n2 = __fmul2_rn(v, pn);
-                                ve[2 * c2] = e2.x;
-                                ve[2 * c2 + 1] = e2.y;
-                                vn[2 * c2] = n2.x;
-                                vn[2 * c2 + 1] = n2.y;
+                                if (MODE == 0) {
+                                    const float2 pe = __ffma2_rn(el1v, dy, __fmul2_rn(el0v, dx));
+                                    const float2 pn = __ffma2_rn(ep2v, dz, __ffma2_rn(ep1v, dy, __fmul2_rn(ep0v, dx)));
+                                    const float2 e2 = __fmul2_rn(v, pe), n2 = __fmul2_rn(v, pn);
+                                    ve[2 * c2] = e2.x;
+                                    ve[2 * c2 + 1] = e2.y;
+                                    vn[2 * c2] = n2.x;
+                                    vn[2 * c2 + 1] = n2.y;
+                                } else {
+                                    // proxy targets: the Cartesian vector val (s - x)
+                                    const float2 x2 = __fmul2_rn(v, dx), y2 = __fmul2_rn(v, dy), z2 = __fmul2_rn(v, dz);
+                                    ve[2 * c2] = x2.x;
+                                    ve[2 * c2 + 1] = x2.y;
+                                    vn[2 * c2] = y2.x;
+                                    vn[2 * c2 + 1] = y2.y;
+                                    vz[2 * c2] = z2.x;
+                                    vz[2 * c2 + 1] = z2.y;
+                                }
                             }
                             // the target itself among these 8 sources: the self pair
                             const int cs = my_pos - (it.off + kStageK * j + 8 * ks);
-                            if (kind == 0 && (unsigned)cs < 8u) {
+                            if (MODE == 0 && kind == 0 && (unsigned)cs < 8u) {
 #pragma unroll
                                 for (int c = 0; c < 8; ++c)
                                     if (c == cs) { ve[c] = self_e; vn[c] = self_n; }
@@ -455,10 +493,22 @@ __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(TcArgs a, int *err
                             const float2 el23 = sub2(make_float2(ve[4 * hh + 2], ve[4 * hh + 3]), make_float2(eh.z, eh.w));
                             const float2 nl01 = sub2(make_float2(vn[4 * hh], vn[4 * hh + 1]), make_float2(nh.x, nh.y));
                             const float2 nl23 = sub2(make_float2(vn[4 * hh + 2], vn[4 * hh + 3]), make_float2(nh.z, nh.w));
-                            *reinterpret_cast<float4 *>(th + oe + 32 * hh) = eh;
-                            *reinterpret_cast<float4 *>(tlo + oe + 32 * hh) = make_float4(el01.x, el01.y, el23.x, el23.y);
-                            *reinterpret_cast<float4 *>(th + on + 32 * hh) = nh;
-                            *reinterpret_cast<float4 *>(tlo + on + 32 * hh) = make_float4(nl01.x, nl01.y, nl23.x, nl23.y);
+                            if (row_in_tile) {
+                                *reinterpret_cast<float4 *>(th + oe + 32 * hh) = eh;
+                                *reinterpret_cast<float4 *>(tlo + oe + 32 * hh) = make_float4(el01.x, el01.y, el23.x, el23.y);
+                                *reinterpret_cast<float4 *>(th + on + 32 * hh) = nh;
+                                *reinterpret_cast<float4 *>(tlo + on + 32 * hh) = make_float4(nl01.x, nl01.y, nl23.x, nl23.y);
+                            }
+                            if (MODE == 1) {
+                                const float4 zh = make_float4(tf32_hi(vz[4 * hh]), tf32_hi(vz[4 * hh + 1]),
+                                                              tf32_hi(vz[4 * hh + 2]), tf32_hi(vz[4 * hh + 3]));
+                                const float2 zl01 = sub2(make_float2(vz[4 * hh], vz[4 * hh + 1]), make_float2(zh.x, zh.y));
+                                const float2 zl23 = sub2(make_float2(vz[4 * hh + 2], vz[4 * hh + 3]), make_float2(zh.z, zh.w));
+                                if (row_in_tile) {
+                                    *reinterpret_cast<float4 *>(th + oz + 32 * hh) = zh;
+                                    *reinterpret_cast<float4 *>(tlo + oz + 32 * hh) = make_float4(zl01.x, zl01.y, zl23.x, zl23.y);
+                                }
+                            }
                         }
                         dev::fence_proxy_async();
                     }
@@ -564,8 +614,9 @@ __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(TcArgs a, int *err
                 if (!(a.items[k].kind & kTcFlush)) continue;
                 wait_bounded(&sm.accfull[cc & 1], (cc >> 1) & 1, abort, err);
                 tc_fence_after();
-                fold_chain(tq + 256 * (cc & 1), &sm.run[0][0], q, lane, k == G.ie - 1, first, G.tgt, G.nt, a.perm,
-                           a.out_x, a.out_y, a.ld_out, a.f0, a.nf, *abort != 0);
+                fold_chain<MODE>(tq + 256 * (cc & 1), &sm.run[0][0], q, lane, k == G.ie - 1, first, G.tgt, G.nt,
+                                 a.perm, a.out_x, a.out_y, a.ld_out, a.f0, a.nf, *abort != 0,
+                                 MODE == 1 ? a.partial + ((size_t)G.out * P + G.row0) * 3 * kF : nullptr);
                 tc_fence_before();
                 __syncwarp();
                 if (lane == 0) mbar_arrive(&sm.accfree[cc & 1]);
@@ -582,7 +633,8 @@ __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(TcArgs a, int *err
     }
 }
 
-// Split weight store: per k-step of 8 store rows, the 64-field rows as one
+// Split weight store (k-steps [k0, k1) of it, with bsrc and bstore offset
+// by the caller): per k-step of 8 store rows, the 64-field rows as one
 // 128-row TF32 tile (field f's hi part at row wrow(f, 0), lo part at
 // wrow(f, 1)) in the canonical no-swizzle K-major layout.  One thread per
 // (k-step, field).
@@ -656,24 +708,29 @@ size_t tc_smem_bytes() {
     return need > 120 * 1024 ? need : 120 * 1024;
 }
 
-void launch_tc_leaf(const TcArgs &a, int nsm, int *err, cudaStream_t st) {
+template <int MODE>
+static void launch_tc(const TcArgs &a, int nsm, int *err, cudaStream_t st) {
     if (a.ngroups <= 0) return;
     const size_t smem = tc_smem_bytes();
     static std::atomic<unsigned long long> done{0};
-    smem_attr_once((const void *)tc_leaf_kernel, (int)smem, done);
+    smem_attr_once((const void *)tc_leaf_kernel<MODE>, (int)smem, done);
     // every SM busy, but no CTA longer than kMaxGroupsPerCta groups, so that
     // kernels of other streams (higher-priority grids) get SMs as CTAs retire
     int grid = (a.ngroups + kMaxGroupsPerCta - 1) / kMaxGroupsPerCta;
     if (grid < nsm) grid = a.ngroups < nsm ? a.ngroups : nsm;
-    tc_leaf_kernel<<<grid, kThreads, smem, st>>>(a, err);
+    tc_leaf_kernel<MODE><<<grid, kThreads, smem, st>>>(a, err);
 }
 
-void launch_split_store(const int32_t *bsrc, int64_t nrows, const float *wF, const float *phiF, float *bstore,
-                        cudaStream_t st) {
-    const int64_t nk = nrows / 8;
+void launch_tc_leaf(const TcArgs &a, int nsm, int *err, cudaStream_t st) { launch_tc<0>(a, nsm, err, st); }
+void launch_tc_proxy(const TcArgs &a, int nsm, int *err, cudaStream_t st) { launch_tc<1>(a, nsm, err, st); }
+
+void launch_split_store(const int32_t *bsrc, int64_t k0, int64_t k1, const float *wF, const float *phiF,
+                        float *bstore, cudaStream_t st) {
+    const int64_t nk = k1 - k0;
     if (nk <= 0) return;
     const int64_t threads = nk * kF;
-    split_store_kernel<<<(unsigned)((threads + 255) / 256), 256, 0, st>>>(bsrc, nk, wF, phiF, bstore);
+    split_store_kernel<<<(unsigned)((threads + 255) / 256), 256, 0, st>>>(bsrc + k0 * 8, nk, wF, phiF,
+                                                                          bstore + k0 * kWStepFloats);
 }
 
 void launch_source_local(const double4 *pool, const int2 *ranges, const double4 *centres, int nranges, float4 *sloc,
