@@ -352,8 +352,8 @@ def main():
         peak = bf16 / 2.0          # dense TF32 = half the bf16 rate
         leaf_flops = 4.0 * F * (st["pairs_pp"] + st["pairs_pc"] + 3.0 * st["macs_down"])
         achieved = leaf_flops / (leaf_ms * 1e-3) / 1e12
-        roof = {"bound": "tensor", "kernel": "tc_leaf_kernel (tcgen05 TF32 hi/lo, M=128 field parts x N=256 target "
-                          "components; PP+PC kernel tiles, DOWN interpolation) + split_store_kernel",
+        roof = {"bound": "tensor", "kernel": "tc_leaf_kernel<0> (tcgen05 TF32 hi/lo, M=128 field parts x N=256 target "
+                          "components; PP+PC kernel tiles, DOWN interpolation) + split_store_kernel (potentials)",
                 "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
                 "peak_source": ("TF32 dense = bf16_tflops/2 of measured" if "bf16_tflops" in peaks else
                                 "TF32 dense = 1.59 PFLOP/s bf16 fallback / 2"),
@@ -402,8 +402,9 @@ def main():
             "e2e": {"value": e2e_val, "unit": "evals/s", "h2d_bytes_per_step": 8 * g.n * F,
                     "d2h_bytes_per_step": 16 * g.n * F, "api": "sal_solve_host (pinned host buffers)"},
             "clocks": clocks,
-            # batched form: prep, upward, finalize, proxy, finalize, split store, leaf per 64-field block
-            "gpu_launches": 7 * args.steps * (((F + 63) // 64) if F > 32 else 1) if form == S.FORM_MIXED else 6 * args.steps,
+            # batched form per 64-field block: prep, split store (points), upward, finalize,
+            # split store (proxies), proxy, finalize, split store (potentials), leaf
+            "gpu_launches": 9 * args.steps * (((F + 63) // 64) if F > 32 else 1) if form == S.FORM_MIXED else 6 * args.steps,
         }
         if cb:
             line["cpu_baseline"] = cb

@@ -64,6 +64,11 @@ struct GridImpl {
     TcItem *tc_items = nullptr;
     MixGroup *tc_proxy_groups = nullptr;
     TcItem *tc_proxy_items = nullptr;
+    MixGroup *tc_up_groups = nullptr;
+    TcItem *tc_up_items = nullptr;
+    int32_t *tc_up_unit_beg = nullptr;
+    float *tc_up_partial = nullptr;
+    float *basis = nullptr;           // upward pass: per-point BLI factors per basis k-step
     int32_t *bsrc = nullptr;
     float *bstore = nullptr;          // split weight store of the tcgen05 leaf pass
     float4 *sloc = nullptr;
@@ -379,6 +384,24 @@ static int ensure_mixed(GridImpl &g, int FT) {
         if (!rc) rc = dupload(g, &g.tc_items, pl.tc_items.data(), pl.tc_items.size());
         if (!rc) rc = dupload(g, &g.tc_proxy_groups, pl.tc_proxy_groups.data(), pl.tc_proxy_groups.size());
         if (!rc) rc = dupload(g, &g.tc_proxy_items, pl.tc_proxy_items.data(), pl.tc_proxy_items.size());
+        if (!rc) rc = dupload(g, &g.tc_up_groups, pl.tc_up_groups.data(), pl.tc_up_groups.size());
+        if (!rc) rc = dupload(g, &g.tc_up_items, pl.tc_up_items.data(), pl.tc_up_items.size());
+        if (!rc) rc = dupload(g, &g.tc_up_unit_beg, pl.tc_up_unit_beg.data(), pl.tc_up_unit_beg.size());
+        const int64_t nbk = (int64_t)pl.tc_bas.size() / 3, nunits = pl.tc_up_unit_beg.empty() ? 0 : pl.tc_up_unit_beg.back();
+        if (!rc) rc = dalloc(g, &g.tc_up_partial, (size_t)nunits * P * FT);
+        if (!rc) rc = dalloc(g, &g.basis, (size_t)nbk * 16 * (pl.d + 1));
+        if (!rc && nbk > 0) {
+            // the basis store, once per grid
+            int32_t *bas = nullptr;
+            CK(cudaMalloc((void **)&bas, pl.tc_bas.size() * sizeof(int32_t)));
+            cudaError_t e = cudaMemcpy(bas, pl.tc_bas.data(), pl.tc_bas.size() * sizeof(int32_t), cudaMemcpyHostToDevice);
+            if (e == cudaSuccess) {
+                mix::launch_basis_store(bas, nbk, g.xieta, g.src_nodes, pl.d + 1, g.basis, g.stream);
+                e = cudaStreamSynchronize(g.stream);
+            }
+            cudaFree(bas);
+            if (e != cudaSuccess) return set_error(SAL_ECUDA, std::string("basis store: ") + cudaGetErrorString(e));
+        }
         if (!rc) rc = dupload(g, &g.bsrc, pl.bsrc.data(), pl.bsrc.size());
         if (!rc) rc = dalloc(g, &g.bstore, pl.bsrc.size() * 2 * (size_t)FT);
         if (!rc) rc = dalloc(g, &g.sloc, n + (size_t)g.nsrc * P);
@@ -440,7 +463,25 @@ static void solve_mixed_block(GridImpl &g, const double *ssh, int64_t ld_ssh, in
     a.ld_out = ld_out;
     a.f0 = f0;
     a.nf = nf;
-    if (!pl.mix_up_groups.empty()) {
+    if (g.bstore) {
+        // 64-field blocks, tcgen05: the points' rows of the split weight store,
+        // then the upward pass; then the proxies' rows
+        mix::launch_split_store(g.bsrc, 0, pl.tc_pt_ksteps, g.wF, g.phiF, g.bstore, st);
+        if (!pl.tc_up_groups.empty()) {
+            mix::TcArgs u{};
+            u.groups = g.tc_up_groups;
+            u.ngroups = (int)pl.tc_up_groups.size();
+            u.items = g.tc_up_items;
+            u.bstore = g.bstore;
+            u.basis = g.basis;
+            u.d = pl.d;
+            u.P = P;
+            u.partial = g.tc_up_partial;
+            mix::launch_tc_upward(u, g.nsm, g.err, st);
+            mix::launch_finalize_mix(g.tc_up_unit_beg, g.tc_up_partial, g.nsrc, P, FT, g.wF + (size_t)n * FT, st);
+        }
+        mix::launch_split_store(g.bsrc, pl.tc_pt_ksteps, pl.tc_src_ksteps, g.wF, g.phiF, g.bstore, st);
+    } else if (!pl.mix_up_groups.empty()) {
         mix::MixArgs u = a;
         u.groups = g.mix_up_groups;
         u.tgt_nodes = g.src_nodes;
@@ -449,9 +490,7 @@ static void solve_mixed_block(GridImpl &g, const double *ssh, int64_t ld_ssh, in
         mix::launch_finalize_mix(g.up_unit_beg, g.mix_up_partial, g.nsrc, P, FT, g.wF + (size_t)n * FT, st);
     }
     if (g.timing) cudaEventRecord(g.ev[1], st);
-    // 64-field blocks: the source rows of the split weight store (points and
-    // proxy weights are final now), then the proxy pass on tcgen05
-    if (g.bstore) mix::launch_split_store(g.bsrc, 0, pl.tc_src_ksteps, g.wF, g.phiF, g.bstore, st);
+    // 64-field blocks: the proxy pass on tcgen05
     if (g.bstore && !pl.tc_proxy_groups.empty()) {
         mix::TcArgs p{};
         p.groups = g.tc_proxy_groups;

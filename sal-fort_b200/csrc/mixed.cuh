@@ -64,10 +64,14 @@ struct TcArgs {
     double *out_x, *out_y;    // caller's outputs (column f at + f*ld_out)
     int64_t ld_out;
     int f0, nf;
-    float *partial;           // proxy pass: per-unit rows (P x 3 components x 64 fields)
+    float *partial;           // proxy / upward pass: per-unit rows (P x components x 64 fields)
+    const float *basis;       // upward pass: BLI factors per basis k-step
 };
 void launch_tc_leaf(const TcArgs &a, int nsm, int *err, cudaStream_t st);
 void launch_tc_proxy(const TcArgs &a, int nsm, int *err, cudaStream_t st);
+void launch_tc_upward(const TcArgs &a, int nsm, int *err, cudaStream_t st);
+void launch_basis_store(const int32_t *bas, int64_t nbk, const double2 *xieta, const double *src_nodes, int n,
+                        float *basis, cudaStream_t st);
 size_t tc_smem_bytes();
 void launch_split_store(const int32_t *bsrc, int64_t k0, int64_t k1, const float *wF, const float *phiF,
                         float *bstore, cudaStream_t st);

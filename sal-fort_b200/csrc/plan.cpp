@@ -353,6 +353,10 @@ bool plan_build(const Tree &t, int d, int mode, const int32_t *list, int64_t nli
     pl->tc_items.clear();
     pl->tc_proxy_items.clear();
     pl->tc_proxy_groups.clear();
+    pl->tc_up_groups.clear();
+    pl->tc_up_items.clear();
+    pl->tc_up_unit_beg.clear();
+    pl->tc_bas.clear();
     pl->bsrc.clear();
     pl->sloc_ranges.clear();
     pl->sloc_centres.clear();
@@ -371,6 +375,7 @@ bool plan_build(const Tree &t, int d, int mode, const int32_t *list, int64_t nli
         int64_t nb = 0;
         for (size_t i = 0; i < leaves.size(); ++i) { leaf_b[i] = nb; nb += up8(t.p[leaves[i]].count()); }
         const int64_t src_b0 = nb, P8 = up8(P), P38 = up8(3 * P);
+        pl->tc_pt_ksteps = src_b0 / 8;
         nb += (int64_t)nsrc * P8;
         const int64_t phi_b0 = nb;
         pl->tc_src_ksteps = phi_b0 / 8;
@@ -468,6 +473,47 @@ bool plan_build(const Tree &t, int d, int mode, const int32_t *list, int64_t nli
                 pl->tc_proxy_groups.push_back(m);
             }
         }
+        // upward pass: per source slot, units of whole leaves of its panel
+        // (at least kUpChunk points, or the panel's rest), rows of at most
+        // kTcRows proxies; every item gets its own k-steps in the basis store
+        pl->tc_up_unit_beg.assign(nsrc + 1, 0);
+        int32_t nunits = 0;
+        int64_t nbk = 0;
+        for (int32_t s = 0; s < nsrc; ++s) {
+            const int ks = pl->src_slot_panel[s];
+            pl->tc_up_unit_beg[s] = nunits;
+            int32_t lb, le;
+            leaf_range(ks, &lb, &le);
+            for (int32_t l = lb; l < le;) {
+                const int64_t b = t.p[leaves[l]].begin;
+                int64_t e = b;
+                int32_t l2 = l;
+                while (l2 < le && e - b < kUpChunk) e = t.p[leaves[l2++]].end;
+                const std::vector<Item> range{Item{(int32_t)b, (int32_t)(e - b), -1, 0}};
+                const int32_t ib = (int32_t)pl->tc_up_items.size();
+                if (!convert(range, 0, 1, ks, pl->tc_up_items)) return false;
+                const int32_t ie = (int32_t)pl->tc_up_items.size();
+                for (int32_t i = ib; i < ie; ++i) {
+                    TcItem &r = pl->tc_up_items[i];
+                    r.row0 = (int32_t)nbk;
+                    for (int32_t k = 0; k < r.cnt; k += 8) {
+                        pl->tc_bas.push_back(s);
+                        pl->tc_bas.push_back(r.off + k);
+                        pl->tc_bas.push_back(std::min(8, r.cnt - k));
+                        ++nbk;
+                    }
+                }
+                for (int32_t r = 0; r < P; r += kTcRows) {
+                    MixGroup m{};
+                    m.tgt = s; m.nt = std::min(kTcRows, P - r); m.ib = ib; m.ie = ie; m.out = nunits; m.row0 = r;
+                    pl->tc_up_groups.push_back(m);
+                }
+                ++nunits;
+                l = l2;
+            }
+        }
+        pl->tc_up_unit_beg[nsrc] = nunits;
+        if (nbk > INT32_MAX / 2) { *err = "grid too large for the basis store"; return false; }
     }
     // ---------------------------------------------------------------- point data in pool order
     pl->pxi.resize(n); pl->peta.resize(n);

@@ -132,6 +132,16 @@ struct Plan {
     // target proxies (row0 = first proxy, out = unit), and their items
     std::vector<MixGroup> tc_proxy_groups;
     std::vector<TcItem> tc_proxy_items;
+    // tcgen05 upward pass: units of whole leaves of a source slot's panel
+    // (tgt = slot, row0 = first proxy, out = unit), items over their points
+    // (row0 = first k-step of the item in the basis store), the first unit
+    // of every slot (nsrc + 1), and per basis k-step (slot, first pool row,
+    // rows) for building the store of per-point BLI factors
+    std::vector<MixGroup> tc_up_groups;
+    std::vector<TcItem> tc_up_items;
+    std::vector<int32_t> tc_up_unit_beg;
+    std::vector<int32_t> tc_bas;                  // 3 per basis k-step
+    int64_t tc_pt_ksteps = 0;                     // k-steps of the store holding points
     std::vector<int32_t> bsrc;
     int64_t tc_src_ksteps = 0;                    // k-steps of the store holding sources (points, proxies)
     // pool row ranges (begin, end) of every leaf and every source slot's

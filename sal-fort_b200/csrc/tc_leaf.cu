@@ -61,7 +61,8 @@ constexpr int kF = 64;                            // fields
 constexpr int kStageK = 16;                       // K columns per stage (two k-steps of 8)
 constexpr int kKStages = 3;                       // kernel-tile ring
 constexpr int kWStages = 4;                       // weight / coordinate ring
-constexpr int kMaxGroupsPerCta = 1;               // CTAs stay short (see launch_tc_leaf)
+constexpr int kMaxGroupsPerCta = 1;
+constexpr int kAuxFloats = 2 * 16 * (kMaxDegree + 1);   // two k-steps of upward factors (covers 2 x 24 coordinates)               // CTAs stay short (see launch_tc_leaf)
 constexpr int kTileFloats = 2048;                 // kernel tile of one k-step: 256 rows x 8, one of hi / lo
 constexpr int kWStepFloats = 1024;                // weight tile of one k-step: 128 rows x 8
 constexpr int kTmemCols = 512;
@@ -79,7 +80,8 @@ constexpr uint32_t kIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(256
 struct TcSmem {
     float Kt[kKStages][2][2][kTileFloats];       // per stage: k-step x {hi, lo} x 256 rows x 8
     float Wt[kWStages][2 * kWStepFloats];        // per stage: 2 k-steps x 128 weight rows x 8
-    float lxyz[kWStages][2][24];                 // per stage and k-step: source x[8], y[8], z[8]
+    float aux[kWStages][kAuxFloats];             // per stage: source x[8] y[8] z[8] per k-step (leaf, proxy)
+                                                 // or BLI factors F[n][8] G[n][8] per k-step (upward)
     float run[2 * kTcRows][kF];                  // running sums: [component x target][field, 16-blocks swapped on odd targets]
     float fx[kTcRows][kMaxDegree + 1];           // per target row: BLI bases in the current DOWN slot
     float fe[kTcRows][kMaxDegree + 1];
@@ -237,6 +239,14 @@ __device__ __forceinline__ void fold_chunk(const float (&x)[16], int c0, float *
             const int ti = __shfl_sync(0xffffffffu, idk, t & 31);
             if (wr && t < nt) out[ti] = (double)v[m];
         }
+    } else if (MODE == 2) {
+        // upward rows: column j is proxy row0 + j; the unit's partial holds
+        // one row of 64 fields per proxy
+#pragma unroll
+        for (int m = 0; m < 8; ++m) {
+            const int j = c0 + 2 * m + odd;
+            if (wr && j < nt) part[(size_t)j * kF + f] = v[m];
+        }
     } else {
         // proxy rows: column j = 85c + r is component c of proxy r; the unit's
         // partial holds (proxy, component) rows of 64 fields
@@ -260,14 +270,14 @@ __device__ __noinline__ void fold_chain(uint32_t td, float *run, int q, int lane
     if (MODE == 0 && end)
 #pragma unroll
         for (int k = 0; k < 4; ++k) idx[k] = 32 * k + lane < nt ? perm[tgt + 32 * k + lane] : 0;
-    const bool wr = end && (MODE == 1 || f0 + f < nf) && !skip;
+    const bool wr = end && (MODE != 0 || f0 + f < nf) && !skip;
     double *ox = MODE == 0 ? out_x + (size_t)(f0 + f) * ld_out : nullptr;
     double *oy = MODE == 0 ? out_y + (size_t)(f0 + f) * ld_out : nullptr;
     // chunks of 16 columns: leaf component ch = c / 128, target slots
     // c % 128 ..+15 (at a group's end only the chunks that hold targets);
     // proxy: all 16 chunks
-    const int per = (MODE == 0 && end) ? (nt + 15) / 16 : 8;
-    const int nchunk = 2 * per;
+    const int per = (MODE != 1 && end) ? (nt + 15) / 16 : 8;
+    const int nchunk = MODE == 2 ? per : 2 * per;   // upward: one component, columns 0..127
     auto col = [&](int i) { return (i / per) * 128 + (i % per) * 16; };
     float xa[16], xb[16];
     tmem_ld16(td + col(0), xa);
@@ -342,7 +352,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(TcArgs a, int *err
         const int oe = canon(MODE == 0 ? row : row, 0) >> 2;
         const int on = canon(MODE == 0 ? kTcRows + row : kTcProxyRows + row, 0) >> 2;
         const int oz = canon(MODE == 0 ? 0 : 2 * kTcProxyRows + row, 0) >> 2;
-        const bool row_in_tile = MODE == 0 || row < kTcProxyRows;
+        const bool row_in_tile = MODE != 1 || row < kTcProxyRows;   // proxy components hold 85 rows
         // wait for a free kernel-tile slot
         auto wait_slot = [&](uint32_t s) {
             if (s >= (uint32_t)kKStages)
@@ -356,7 +366,10 @@ __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(TcArgs a, int *err
             // the row's target relative to the leaf centre and its east /
             // north unit vectors (zero at the poles, as the reference's guard)
             float tl0 = 0.f, tl1 = 0.f, tl2 = 0.f, el0 = 0.f, el1 = 0.f, ep0 = 0.f, ep1 = 0.f, ep2 = 0.f;
-            if (rvalid) {
+            // upward: this row's proxy p = row0 + row = up_i + up_j n
+            const int up_p = MODE == 2 ? G.row0 + (rvalid ? row : 0) : 0;
+            const int up_i = up_p % n, up_j = up_p / n;
+            if (MODE != 2 && rvalid) {
                 // leaf: the pool point; proxy: proxy row0 + row of target slot G.tgt
                 const double4 c = MODE == 0 ? a.tgt[G.tgt + row] : a.tgt[(size_t)G.tgt * P + G.row0 + row];
                 tl0 = (float)(c.x - G.cx);
@@ -421,7 +434,20 @@ __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(TcArgs a, int *err
                     const uint32_t slot = st % kKStages;
                     if (active) {
                         float ve[8], vn[8], vz[8];
-                        if (MODE == 0 && kind == 2) {
+                        if (MODE == 2) {
+                            // upward: the BLI basis of proxy (i, j) at the 8 points,
+                            // F_i(xi) G_j(eta) from the per-point factors
+                            wait_bounded(&sm.wfull[st % kWStages], (st / kWStages) & 1, abort, err);
+                            const float *Fb = sm.aux[st % kWStages] + 16 * n * ks;
+                            const float4 f0 = *reinterpret_cast<const float4 *>(Fb + 8 * up_i);
+                            const float4 f1 = *reinterpret_cast<const float4 *>(Fb + 8 * up_i + 4);
+                            const float4 g0 = *reinterpret_cast<const float4 *>(Fb + 8 * n + 8 * up_j);
+                            const float4 g1 = *reinterpret_cast<const float4 *>(Fb + 8 * n + 8 * up_j + 4);
+                            ve[0] = f0.x * g0.x; ve[1] = f0.y * g0.y; ve[2] = f0.z * g0.z; ve[3] = f0.w * g0.w;
+                            ve[4] = f1.x * g1.x; ve[5] = f1.y * g1.y; ve[6] = f1.z * g1.z; ve[7] = f1.w * g1.w;
+#pragma unroll
+                            for (int c = 0; c < 8; ++c) vn[c] = 0.f;
+                        } else if (MODE == 0 && kind == 2) {
                             // DOWN: BLI basis of the target x its unit vector's
                             // component of the Cartesian row
                             const int *km0 = sm.kmap + it.row0 + kStageK * j + 8 * ks;
@@ -438,7 +464,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(TcArgs a, int *err
                             // PP / PC: kernel value x projected displacement,
                             // two columns per packed instruction
                             wait_bounded(&sm.wfull[st % kWStages], (st / kWStages) & 1, abort, err);
-                            const float *L = sm.lxyz[st % kWStages][ks];
+                            const float *L = sm.aux[st % kWStages] + 24 * ks;
 #pragma unroll
                             for (int c2 = 0; c2 < 4; ++c2) {
                                 const float2 dx = sub2(*reinterpret_cast<const float2 *>(L + 2 * c2), tx2);
@@ -496,8 +522,10 @@ __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(TcArgs a, int *err
                             if (row_in_tile) {
                                 *reinterpret_cast<float4 *>(th + oe + 32 * hh) = eh;
                                 *reinterpret_cast<float4 *>(tlo + oe + 32 * hh) = make_float4(el01.x, el01.y, el23.x, el23.y);
-                                *reinterpret_cast<float4 *>(th + on + 32 * hh) = nh;
-                                *reinterpret_cast<float4 *>(tlo + on + 32 * hh) = make_float4(nl01.x, nl01.y, nl23.x, nl23.y);
+                                if (MODE != 2) {
+                                    *reinterpret_cast<float4 *>(th + on + 32 * hh) = nh;
+                                    *reinterpret_cast<float4 *>(tlo + on + 32 * hh) = make_float4(nl01.x, nl01.y, nl23.x, nl23.y);
+                                }
                             }
                             if (MODE == 1) {
                                 const float4 zh = make_float4(tf32_hi(vz[4 * hh]), tf32_hi(vz[4 * hh + 1]),
@@ -581,11 +609,15 @@ __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(TcArgs a, int *err
                     if (lane == 0) {
                         const int ncol = min(kStageK, it.cnt - kStageK * j), nks = (ncol + 7) >> 3;
                         const uint32_t wbytes = (uint32_t)nks * kWStepFloats * 4;
-                        const uint32_t lbytes = (it.kind & 3) != 2 ? (uint32_t)nks * 96 : 0u;
+                        const uint32_t lbytes = MODE == 2 ? (uint32_t)nks * 64 * n
+                                                : ((it.kind & 3) != 2 ? (uint32_t)nks * 96 : 0u);
                         dev::mbar_expect_tx(&sm.wfull[jb], wbytes + lbytes);
                         if (!*abort) {
-                            if (lbytes)
-                                dev::bulk_g2s(sm.lxyz[jb], a.sxyz + (size_t)(it.kb + 2 * j) * 24, lbytes, &sm.wfull[jb]);
+                            if (lbytes) {
+                                const float *src = MODE == 2 ? a.basis + (size_t)(it.row0 + 2 * j) * 16 * n
+                                                             : a.sxyz + (size_t)(it.kb + 2 * j) * 24;
+                                dev::bulk_g2s(sm.aux[jb], src, lbytes, &sm.wfull[jb]);
+                            }
                             dev::bulk_g2s(sm.Wt[jb], a.bstore + (size_t)(it.kb + 2 * j) * kWStepFloats, wbytes,
                                           &sm.wfull[jb]);
                         }
@@ -616,7 +648,9 @@ __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(TcArgs a, int *err
                 tc_fence_after();
                 fold_chain<MODE>(tq + 256 * (cc & 1), &sm.run[0][0], q, lane, k == G.ie - 1, first, G.tgt, G.nt,
                                  a.perm, a.out_x, a.out_y, a.ld_out, a.f0, a.nf, *abort != 0,
-                                 MODE == 1 ? a.partial + ((size_t)G.out * P + G.row0) * 3 * kF : nullptr);
+                                 MODE == 1   ? a.partial + ((size_t)G.out * P + G.row0) * 3 * kF
+                                 : MODE == 2 ? a.partial + ((size_t)G.out * P + G.row0) * kF
+                                             : nullptr);
                 tc_fence_before();
                 __syncwarp();
                 if (lane == 0) mbar_arrive(&sm.accfree[cc & 1]);
@@ -687,6 +721,31 @@ __global__ void source_ksteps_kernel(const int32_t *__restrict__ bsrc, int64_t n
     sxyz[ks * 24 + 16 + i] = p.z;
 }
 
+// Basis store of the upward pass: per k-step b of an upward item (slot s,
+// pool rows first..first+cnt-1), the FP64 BLI factors of its 8 points over the
+// slot panel's nodes, rounded to FP32: F[i][8] (xi nodes) then G[j][8] (eta
+// nodes); zero for padding rows.  One thread per (k-step, point).
+__global__ void basis_store_kernel(const int32_t *__restrict__ bas, int64_t nbk, const double2 *__restrict__ xieta,
+                                   const double *__restrict__ src_nodes, int n, float *__restrict__ basis) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nbk * 8) return;
+    const int64_t b = t >> 3;
+    const int i = (int)(t & 7);
+    const int s = bas[3 * b], first = bas[3 * b + 1], cnt = bas[3 * b + 2];
+    float *F = basis + b * 16 * n, *G = F + 8 * n;
+    if (i >= cnt) {
+        for (int k = 0; k < n; ++k) F[8 * k + i] = G[8 * k + i] = 0.f;
+        return;
+    }
+    const double2 e = xieta[first + i];
+    const double *nodes = src_nodes + (size_t)s * 2 * n;
+    double f[kMaxDegree + 1];
+    dev::bli_basis(e.x, nodes, n, f);
+    for (int k = 0; k < n; ++k) F[8 * k + i] = (float)f[k];
+    dev::bli_basis(e.y, nodes + n, n, f);
+    for (int k = 0; k < n; ++k) G[8 * k + i] = (float)f[k];
+}
+
 // Per pool point, the self pair of sal_grad_gfunc (fast_sum_module.f90:9-31)
 // in FP64 divided by the kernel constant: the leaf epilogue multiplies it by
 // the point's FP32 weight row, which carries the constant.
@@ -723,6 +782,7 @@ static void launch_tc(const TcArgs &a, int nsm, int *err, cudaStream_t st) {
 
 void launch_tc_leaf(const TcArgs &a, int nsm, int *err, cudaStream_t st) { launch_tc<0>(a, nsm, err, st); }
 void launch_tc_proxy(const TcArgs &a, int nsm, int *err, cudaStream_t st) { launch_tc<1>(a, nsm, err, st); }
+void launch_tc_upward(const TcArgs &a, int nsm, int *err, cudaStream_t st) { launch_tc<2>(a, nsm, err, st); }
 
 void launch_split_store(const int32_t *bsrc, int64_t k0, int64_t k1, const float *wF, const float *phiF,
                         float *bstore, cudaStream_t st) {
@@ -740,6 +800,12 @@ void launch_source_local(const double4 *pool, const int2 *ranges, const double4 
 
 void launch_source_ksteps(const int32_t *bsrc, int64_t nks, const float4 *sloc, float *sxyz, cudaStream_t st) {
     if (nks > 0) source_ksteps_kernel<<<(unsigned)((nks * 8 + 255) / 256), 256, 0, st>>>(bsrc, nks, sloc, sxyz);
+}
+
+void launch_basis_store(const int32_t *bas, int64_t nbk, const double2 *xieta, const double *src_nodes, int n,
+                        float *basis, cudaStream_t st) {
+    if (nbk > 0)
+        basis_store_kernel<<<(unsigned)((nbk * 8 + 255) / 256), 256, 0, st>>>(bas, nbk, xieta, src_nodes, n, basis);
 }
 
 void launch_self_pair(const double4 *pool, int n, double2 *selfk, cudaStream_t st) {

@@ -85,3 +85,24 @@ def test_tcgen05_leaf_pass_matches_mma_sync_leaf_pass():
     g64.sync()
     for f in range(6):
         assert rel_l2(bx[f].cpu().numpy(), by[f].cpu().numpy(), ax[f].cpu().numpy(), ay[f].cpu().numpy()) <= 2e-6
+
+
+@pytest.mark.parametrize("degree", [9, 12])
+def test_tcgen05_passes_at_other_degrees(degree):
+    """P = (d+1)^2 = 100 and 169 proxies: the upward pass's groups cover more
+    than 85 and more than 128 proxy rows, the proxy pass's groups are cut in
+    85-row chunks.  The batched form stays within 5e-6 of the FP64 accurate
+    form (and has no NaN from tile rows left unwritten)."""
+    torch = _torch()
+    import salgpu as S
+    g, hs = grid_and_ssh("small_3000", nfields=3, seed=6)
+    t = S.tree_traverse(g.xs, g.ys, g.zs, g.n, 20)
+    L = S.dual_tree_traversal(t, 0.7, 20)
+    grid = S.Grid(t, g.xs, g.ys, g.zs, g.areas, degree, S.MODE_DTT, L, max_fields=64)
+    ssh = torch.tensor(hs, device="cuda")
+    mx, my = grid.solve(ssh, form=S.FORM_MIXED)
+    ax, ay = grid.solve(ssh, form=S.FORM_ACCURATE)
+    torch.cuda.synchronize()
+    assert not (torch.isnan(mx).any() or torch.isnan(my).any())
+    for f in range(3):
+        assert rel_l2(mx[f].cpu().numpy(), my[f].cpu().numpy(), ax[f].cpu().numpy(), ay[f].cpu().numpy()) <= 5e-6
