@@ -195,8 +195,12 @@ def serving_run(args, S, torch, dev):
     for name in sizes:
         srv.submit(serve.Request(name, pools[name][:2]))
     srv.run_until_idle()
-    for name in sizes:                       # warm each grid's full-width batch too
-        srv.submit(serve.Request(name, pools[name][:16]))
+    # warm every request shape (1-16 fields) on every grid, so that the
+    # device allocator has cached blocks for the results before the clock starts
+    for k in range(1, 17):
+        for name in sizes:
+            srv.submit(serve.Request(name, pools[name][:k]))
+        srv.run_until_idle()
     srv.run_until_idle()
     t0 = time.perf_counter()
     reqs = serve.run_workload(srv, pools, weights, args.serve_rate, args.serve_seconds, seed=7, keep=2)

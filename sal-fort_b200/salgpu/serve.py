@@ -35,6 +35,7 @@ tests/test_serve.py checks.
 """
 from __future__ import annotations
 
+import gc
 import itertools
 import time
 from collections import OrderedDict, deque
@@ -402,6 +403,19 @@ def run_workload(server: Server, pools: dict, weights: dict, rate: float, durati
             idx = torch.as_tensor(idx, device=pool.device)
         plan.append((t, name, idx))
     reqs = []
+    # the loop is single-threaded: a cyclic-garbage pass in the middle of it
+    # would stall every grid's batching at once
+    gc_was = gc.isenabled()
+    gc.disable()
+    try:
+        _replay(server, plan, pools, gen, keep, reqs)
+    finally:
+        if gc_was:
+            gc.enable()
+    return reqs
+
+
+def _replay(server: Server, plan: list, pools: dict, gen, keep, reqs: list) -> None:
     t0 = server.clock()
     i = 0
     seen, kept = len(server.completed), {}
@@ -426,7 +440,6 @@ def run_workload(server: Server, pools: dict, weights: dict, rate: float, durati
                 reqs.append(server.submit(Request(name, x, arrival=t0 + t, ready=ev)))
             i += 1
         server.step()
-    return reqs
 
 
 def summarize(reqs: list, cells: dict, wall: float, batches: list | None = None) -> dict:
