@@ -23,13 +23,17 @@
 //               split into TF32 hi + lo, stored to shared memory in the
 //               canonical K-major layout (the MMA's B operand).  The self
 //               pair enters as the tile's diagonal entry: the reference
-//               kernel's FP64 value at distance zero (rounding noise).
+//               kernel's FP64 value at distance zero (rounding noise).  The
+//               sources' FP32 coordinates (per k-step x[8] y[8] z[8]) are
+//               read from global memory into registers a stage ahead: a
+//               stage is bound by the latency of its shared-memory round
+//               trips (barrier polls, loads, the proxy fence), not by its
+//               arithmetic, so each one taken off the chain counts.
 //   warp 8      issues the MMAs.
 //   warp 9      loads, per stage, the weight tiles (pre-split TF32 hi / lo,
-//               written once per solve by split_store_kernel) and the sources'
-//               FP32 coordinates (per k-step x[8] y[8] z[8], so that column
-//               pairs load as float2 for the packed FP32x2 arithmetic) with
-//               bulk copies into a 4-deep ring.
+//               written once per solve by split_store_kernel), and for the
+//               upward pass the BLI factors, with bulk copies into a 4-deep
+//               ring.
 //   warps 10-13 fold finished accumulator chains into the running sums and
 //               write the outputs (warp w: tensor memory lanes 32(w%4)..+31).
 // The tensor cores accumulate with truncation, so one chain over all of a
@@ -52,17 +56,18 @@ using dev::smem_u32;
 namespace {
 
 constexpr int kProdWarps = 8;
-constexpr int kProducers = kProdWarps * 32;      // one per (target row, k-step of a stage)
+constexpr int kProducers = kProdWarps * 32;
 constexpr int kMmaWarp = kProdWarps;
 constexpr int kLoadWarp = kProdWarps + 1;
 constexpr int kFoldWarps = 4;                     // one per tensor memory lane quarter
 constexpr int kThreads = (kProdWarps + 2 + kFoldWarps) * 32;   // 448
 constexpr int kF = 64;                            // fields
-constexpr int kStageK = 16;                       // K columns per stage (two k-steps of 8)
-constexpr int kKStages = 3;                       // kernel-tile ring
-constexpr int kWStages = 4;                       // weight / coordinate ring
-constexpr int kMaxGroupsPerCta = 1;
-constexpr int kAuxFloats = 2 * 16 * (kMaxDegree + 1);   // two k-steps of upward factors (covers 2 x 24 coordinates)               // CTAs stay short (see launch_tc_leaf)
+constexpr int kStageK = 32;                       // K columns per stage (four k-steps of 8)
+constexpr int kStageKs = kStageK / 8;             // k-steps per stage
+constexpr int kKStages = 2;                       // kernel-tile ring
+constexpr int kWStages = 3;                       // weight / upward-factor ring
+constexpr int kMaxGroupsPerCta = 1;               // CTAs stay short (see launch_tc)
+constexpr int kAuxFloats = kStageKs * 16 * (kMaxDegree + 1);   // upward factors of a stage's k-steps
 constexpr int kTileFloats = 2048;                 // kernel tile of one k-step: 256 rows x 8, one of hi / lo
 constexpr int kWStepFloats = 1024;                // weight tile of one k-step: 128 rows x 8
 constexpr int kTmemCols = 512;
@@ -78,15 +83,13 @@ constexpr uint32_t kIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(256
                             ((uint32_t)(128 >> 4) << 24);
 
 struct TcSmem {
-    float Kt[kKStages][2][2][kTileFloats];       // per stage: k-step x {hi, lo} x 256 rows x 8
-    float Wt[kWStages][2 * kWStepFloats];        // per stage: 2 k-steps x 128 weight rows x 8
-    float aux[kWStages][kAuxFloats];             // per stage: source x[8] y[8] z[8] per k-step (leaf, proxy)
-                                                 // or BLI factors F[n][8] G[n][8] per k-step (upward)
-    float run[2 * kTcRows][kF];                  // running sums: [component x target][field, 16-blocks swapped on odd targets]
-    float fx[kTcRows][kMaxDegree + 1];           // per target row: BLI bases in the current DOWN slot
+    float Kt[kKStages][kStageKs][2][kTileFloats];   // per stage: k-step x {hi, lo} x 256 rows x 8
+    float Wt[kWStages][kStageKs * kWStepFloats];    // per stage: k-steps x 128 weight rows x 8
+    float aux[kWStages][kAuxFloats];                // per stage: BLI factors F[n][8] G[n][8] per k-step (upward)
+    float fx[kTcRows][kMaxDegree + 1];              // per target row: BLI bases in the current DOWN slot
     float fe[kTcRows][kMaxDegree + 1];
     int kmap[kKmap];
-    uint64_t kfull[kKStages], kempty[kKStages], wfull[kWStages], wempty[kWStages], accfull[2], accfree[2], fin;
+    uint64_t kfull[kKStages], kempty[kKStages], wfull[kWStages], wempty[kWStages], accfull, accfree, fin;
     uint32_t tmem_base;
     int abort;
 };
@@ -122,11 +125,15 @@ __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 // Bounded wait on an mbarrier phase; on time-out raises the error flag and
-// the CTA-wide abort flag (later waits then return at once).
+// the CTA-wide abort flag (later waits then give up after one poll).  A phase
+// that has already completed costs one poll and no read of the flag: every
+// shared-memory round trip is on the producers' critical path.
 __device__ __forceinline__ void wait_bounded(uint64_t *bar, uint32_t parity, volatile int *abort, int *err) {
-    if (*abort) return;
-    for (uint32_t it = 0; it < kWaitPolls; ++it)
+    if (dev::mbar_try_wait(bar, parity)) return;
+    for (uint32_t it = 0; it < kWaitPolls; ++it) {
+        if (*abort) return;
         if (dev::mbar_try_wait(bar, parity)) return;
+    }
     *abort = 1;
     atomicExch(err, dev::kErrTimeout);
 }
@@ -178,6 +185,18 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
     for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+__device__ __forceinline__ void tmem_st16(uint32_t taddr, const float (&v)[16]) {
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15, %16};" ::"r"(taddr),
+        "r"(__float_as_uint(v[0])), "r"(__float_as_uint(v[1])), "r"(__float_as_uint(v[2])), "r"(__float_as_uint(v[3])),
+        "r"(__float_as_uint(v[4])), "r"(__float_as_uint(v[5])), "r"(__float_as_uint(v[6])), "r"(__float_as_uint(v[7])),
+        "r"(__float_as_uint(v[8])), "r"(__float_as_uint(v[9])), "r"(__float_as_uint(v[10])),
+        "r"(__float_as_uint(v[11])), "r"(__float_as_uint(v[12])), "r"(__float_as_uint(v[13])),
+        "r"(__float_as_uint(v[14])), "r"(__float_as_uint(v[15]))
+        : "memory");
+}
+__device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
 
 // BLI basis (FP64, stored as FP32) of one coordinate of a target over one
 // axis's Chebyshev nodes.  Out of line: its local array stays out of the
@@ -200,70 +219,54 @@ __host__ __device__ constexpr int wrow(int f, int part) { return 32 * (f >> 4) +
 
 }  // namespace
 
-// Folds a finished accumulator chain (warp-collective; this warp's lane
-// quarter q: fields 16q..16q+15 of both components for the group's 128
-// target slots).  Lanes 0-15 hold the chain's hi rows, lanes 16-31 the same
-// fields' lo rows; per column pair, lanes 0-15 take the even column and lanes
-// 16-31 the odd one, so hi + lo of a field meet in one lane.  Mid-group:
-// running sum (+)= chain (the group's first chain stores).  At the group's
-// end: running sum + chain to the caller's outputs for its nt targets.
-// Tensor memory loads are double-buffered and each 16-column chunk reads its
-// 8 running-sum entries before it writes any, so the chunk's latencies overlap.
+// Writes one finished 16-column chunk x (this lane's accumulator row, the
+// running sum already added) to its destination at a group's end.  Lanes
+// 0-15 hold fields' hi rows, lanes 16-31 the same fields' lo rows; per
+// column pair, lanes 0-15 write the even column and lanes 16-31 the odd one,
+// so hi + lo of a field meet in one lane.
 template <int MODE>
-__device__ __forceinline__ void fold_chunk(const float (&x)[16], int c0, float *run, int f, int odd, bool end,
-                                           bool first, int nt, int idk, double *out, bool wr, float *part) {
-    float v[8], rs[8];
-    float *rp[8];
+__device__ __forceinline__ void emit_chunk(const float (&x)[16], int c0, int f, int odd, int nt, int idk, double *out,
+                                           bool wr, float *part) {
 #pragma unroll
     for (int m = 0; m < 8; ++m) {
         const float lo_even = __shfl_down_sync(0xffffffffu, x[2 * m], 16);
         const float hi_odd = __shfl_up_sync(0xffffffffu, x[2 * m + 1], 16);
-        v[m] = odd ? x[2 * m + 1] + hi_odd : x[2 * m] + lo_even;
-        // odd target slots store their fields with the 16-blocks swapped,
-        // so the two half-warps hit different banks
-        rp[m] = run + (size_t)(c0 + 2 * m + odd) * kF + (f ^ (odd << 4));
-    }
-    if (!first) {
-#pragma unroll
-        for (int m = 0; m < 8; ++m) rs[m] = *rp[m];
-#pragma unroll
-        for (int m = 0; m < 8; ++m) v[m] += rs[m];
-    }
-    if (!end) {
-#pragma unroll
-        for (int m = 0; m < 8; ++m) *rp[m] = v[m];
-    } else if (MODE == 0) {
-#pragma unroll
-        for (int m = 0; m < 8; ++m) {
-            const int t = (c0 & 127) + 2 * m + odd;
+        const int j = c0 + 2 * m + odd;   // column
+        if (MODE == 0) {
+            const int t = j & 127;
             const int ti = __shfl_sync(0xffffffffu, idk, t & 31);
-            if (wr && t < nt) out[ti] = (double)v[m];
-        }
-    } else if (MODE == 2) {
-        // upward rows: column j is proxy row0 + j; the unit's partial holds
-        // one row of 64 fields per proxy
-#pragma unroll
-        for (int m = 0; m < 8; ++m) {
-            const int j = c0 + 2 * m + odd;
-            if (wr && j < nt) part[(size_t)j * kF + f] = v[m];
-        }
-    } else {
-        // proxy rows: column j = 85c + r is component c of proxy r; the unit's
-        // partial holds (proxy, component) rows of 64 fields
-#pragma unroll
-        for (int m = 0; m < 8; ++m) {
-            const int j = c0 + 2 * m + odd, c = j / kTcProxyRows, r = j - c * kTcProxyRows;
-            if (wr && c < 3 && r < nt) part[((size_t)r * 3 + c) * kF + f] = v[m];
+            const double v = odd ? (double)hi_odd + (double)x[2 * m + 1] : (double)x[2 * m] + (double)lo_even;
+            if (wr && t < nt) out[ti] = v;
+        } else {
+            const float v = odd ? hi_odd + x[2 * m + 1] : x[2 * m] + lo_even;
+            if (MODE == 2) {
+                // upward rows: column j is proxy row0 + j; the unit's partial
+                // holds one row of 64 fields per proxy
+                if (wr && j < nt) part[(size_t)j * kF + f] = v;
+            } else {
+                // proxy rows: column j = 85c + r is component c of proxy r; the
+                // unit's partial holds (proxy, component) rows of 64 fields
+                const int c = j / kTcProxyRows, r = j - c * kTcProxyRows;
+                if (wr && c < 3 && r < nt) part[((size_t)r * 3 + c) * kF + f] = v;
+            }
         }
     }
 }
 
+// Folds a finished accumulator chain (warp-collective; this warp's lane
+// quarter q: fields 16q..16q+15, hi rows in lanes 0-15 and lo rows in lanes
+// 16-31, for the group's 256 columns).  The running sums live in tensor
+// memory next to the accumulator (columns 256-511, same row layout), hi and
+// lo rows apart: mid-group, running sum (+)= chain with round-to-nearest FP32
+// adds (the group's first chain stores); at the group's end, running sum +
+// chain goes to the caller's outputs, hi + lo added in FP64.
 // MODE 0 (leaf): columns 128c + t are component c (east, north) of target t,
 // ends go to the caller's outputs.  MODE 1 (proxy): columns 85c + r are
 // Cartesian component c of proxy r, ends go to the unit's partial rows `part`.
+// MODE 2 (upward): columns j < 128 are proxies row0 + j.
 template <int MODE>
-__device__ __noinline__ void fold_chain(uint32_t td, float *run, int q, int lane, bool end, bool first, int tgt,
-                                        int nt, const int32_t *__restrict__ perm, double *out_x, double *out_y,
+__device__ __noinline__ void fold_chain(uint32_t td, int q, int lane, bool end, bool first, int tgt, int nt,
+                                        const int32_t *__restrict__ perm, double *out_x, double *out_y,
                                         int64_t ld_out, int f0, int nf, bool skip, float *part) {
     const int f = 16 * q + (lane & 15), odd = lane >> 4;
     int idx[4] = {0, 0, 0, 0};   // caller index of target slot 32k + lane
@@ -279,25 +282,26 @@ __device__ __noinline__ void fold_chain(uint32_t td, float *run, int q, int lane
     const int per = (MODE != 1 && end) ? (nt + 15) / 16 : 8;
     const int nchunk = MODE == 2 ? per : 2 * per;   // upward: one component, columns 0..127
     auto col = [&](int i) { return (i / per) * 128 + (i % per) * 16; };
-    float xa[16], xb[16];
-    tmem_ld16(td + col(0), xa);
+    float x[16], r[16];
 #pragma unroll 1
-    for (int i = 0; i < nchunk; i += 2) {
+    for (int i = 0; i < nchunk; ++i) {
+        const int c = col(i);
+        tmem_ld16(td + c, x);
+        if (!first) tmem_ld16(td + 256 + c, r);
         tmem_wait_ld();
-        if (i + 1 < nchunk) tmem_ld16(td + col(i + 1), xb);
-        {
-            const int c = col(i), ik = (c & 127) >> 5;
-            const int idk = ik == 0 ? idx[0] : ik == 1 ? idx[1] : ik == 2 ? idx[2] : idx[3];
-            fold_chunk<MODE>(xa, c, run, f, odd, end, first, nt, idk, c < 128 ? ox : oy, wr, part);
+        if (!first) {
+#pragma unroll
+            for (int m = 0; m < 16; ++m) x[m] += r[m];
         }
-        if (i + 1 < nchunk) {
-            tmem_wait_ld();
-            if (i + 2 < nchunk) tmem_ld16(td + col(i + 2), xa);
-            const int c = col(i + 1), ik = (c & 127) >> 5;
+        if (!end) {
+            tmem_st16(td + 256 + c, x);
+        } else {
+            const int ik = (c & 127) >> 5;
             const int idk = ik == 0 ? idx[0] : ik == 1 ? idx[1] : ik == 2 ? idx[2] : idx[3];
-            fold_chunk<MODE>(xb, c, run, f, odd, end, first, nt, idk, c < 128 ? ox : oy, wr, part);
+            emit_chunk<MODE>(x, c, f, odd, nt, idk, c < 128 ? ox : oy, wr, part);
         }
     }
+    if (!end) tmem_wait_st();
 }
 
 template <int MODE>
@@ -325,10 +329,8 @@ __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(TcArgs a, int *err
             dev::mbar_init(&sm.wfull[j], 1);
             dev::mbar_init(&sm.wempty[j], 1);
         }
-        for (int j = 0; j < 2; ++j) {
-            dev::mbar_init(&sm.accfull[j], 1);
-            dev::mbar_init(&sm.accfree[j], kFoldWarps);
-        }
+        dev::mbar_init(&sm.accfull, 1);
+        dev::mbar_init(&sm.accfree, kFoldWarps);
         dev::mbar_init(&sm.fin, 1);
         dev::fence_mbar_init();
         sm.abort = 0;
@@ -346,23 +348,51 @@ __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(TcArgs a, int *err
 
     if (warp < kProdWarps) {
         // ============================================================ producers
-        const int row = tid & (kTcRows - 1), ks = tid >> 7;      // generation: target row, k-step of the stage
-        // canonical offsets (floats) of this thread's rows in a kernel tile:
-        // leaf east / north at rows t, 128 + t; proxy x / y / z at 85c + r
-        const int oe = canon(MODE == 0 ? row : row, 0) >> 2;
-        const int on = canon(MODE == 0 ? kTcRows + row : kTcProxyRows + row, 0) >> 2;
-        const int oz = canon(MODE == 0 ? 0 : 2 * kTcProxyRows + row, 0) >> 2;
-        const bool row_in_tile = MODE != 1 || row < kTcProxyRows;   // proxy components hold 85 rows
-        // wait for a free kernel-tile slot
-        auto wait_slot = [&](uint32_t s) {
-            if (s >= (uint32_t)kKStages)
-                wait_bounded(&sm.kempty[s % kKStages], ((s / kKStages) - 1) & 1, abort, err);
+        // A stage's tasks are (row block of 32 targets, k-step) pairs, one
+        // 8-source k-step of 32 rows each.  A stage costs the latency of the
+        // busiest warp's tasks, so the tasks of small groups (one or two
+        // row blocks: the second tile of a leaf with more than 128 points)
+        // are spread over all warps:
+        //   3-4 row blocks: warp w takes row block w % 4, k-steps w / 4, w / 4 + 2
+        //   2 row blocks:   warp w takes row block w % 2, k-step w / 2
+        //   1 row block:    warp w < 4 takes k-step w (warps 4-7 only arrive)
+        // Source coordinates of k-step kk of stage jj of item x (x[8] y[8]
+        // z[8] in the per-k-step store), or null where the item has no such
+        // k-step or no point sources.  The leaf and proxy passes read them
+        // from global memory into registers one task ahead, so no
+        // shared-memory round trip sits between the slot check and the
+        // arithmetic.
+        auto kptr = [&](const TcItem &x, int jj, int kk) -> const float4 * {
+            const int ki = kStageKs * jj + kk;
+            return (MODE != 2 && (x.kind & 3) != 2 && 8 * ki < x.cnt)
+                       ? reinterpret_cast<const float4 *>(a.sxyz + (size_t)(x.kb + ki) * 24)
+                       : nullptr;
+        };
+        float4 pre[6] = {};
+        const float4 *pre_src = nullptr;   // where pre was loaded from
+        auto fetch = [&](const float4 *p) {
+            if (p) {
+#pragma unroll
+                for (int i = 0; i < 6; ++i) pre[i] = __ldg(p + i);
+            }
+            pre_src = p;
         };
 
         for (int gi = blockIdx.x; gi < a.ngroups; gi += gridDim.x) {
             const MixGroup G = a.groups[gi];
             const int ni = G.ie - G.ib;
-            const bool active = (row & ~31) < G.nt, rvalid = row < G.nt;
+            const int rb = (G.nt + 31) >> 5;
+            const int wb = rb >= 3 ? (warp & 3) : rb == 2 ? (warp & 1) : 0;            // row block
+            const int kfirst = rb >= 3 ? (warp >> 2) : rb == 2 ? (warp >> 1) : warp;    // first k-step
+            const int kstride = rb >= 3 ? 2 : kStageKs;
+            const int row = 32 * wb + lane;
+            const bool active = 32 * wb < G.nt, rvalid = row < G.nt;
+            // canonical offsets (floats) of this thread's rows in a kernel tile:
+            // leaf east / north at rows t, 128 + t; proxy x / y / z at 85c + r
+            const int oe = canon(row, 0) >> 2;
+            const int on = canon(MODE == 0 ? kTcRows + row : kTcProxyRows + row, 0) >> 2;
+            const int oz = canon(MODE == 0 ? 0 : 2 * kTcProxyRows + row, 0) >> 2;
+            const bool row_in_tile = MODE != 1 || row < kTcProxyRows;   // proxy components hold 85 rows
             // the row's target relative to the leaf centre and its east /
             // north unit vectors (zero at the poles, as the reference's guard)
             float tl0 = 0.f, tl1 = 0.f, tl2 = 0.f, el0 = 0.f, el1 = 0.f, ep0 = 0.f, ep1 = 0.f, ep2 = 0.f;
@@ -385,9 +415,9 @@ __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(TcArgs a, int *err
                 }
             }
             if (ni == 0) {
-                // no sources: the self pair alone
-                if (MODE == 0 && rvalid && ks == 0 && !*abort) {
-                    const int pos = G.tgt + row, idx = a.perm[pos];
+                // no sources: the self pair alone (thread t: target t)
+                if (MODE == 0 && tid < G.nt && !*abort) {
+                    const int pos = G.tgt + tid, idx = a.perm[pos];
                     const double2 sk = a.selfk[pos];
                     for (int f = 0; f < kF && a.f0 + f < a.nf; ++f) {
                         const double w = (double)a.wF[(size_t)pos * kF + f];
@@ -410,6 +440,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(TcArgs a, int *err
             // item records are read one item ahead, so their latency hides
             // behind the current item's stages
             TcItem nxt = a.items[G.ib];
+            if (active) fetch(kptr(nxt, 0, kfirst));
             for (int k = 0; k < ni; ++k) {
                 const TcItem it = nxt;
                 if (k + 1 < ni) nxt = a.items[G.ib + k + 1];
@@ -417,28 +448,39 @@ __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(TcArgs a, int *err
                 const int nst = (it.cnt + kStageK - 1) / kStageK;
                 if (MODE == 0 && kind == 2 && it.off != cur_slot) {
                     // BLI bases of every target row in the new slot: thread
-                    // (row, 0) the xi basis, thread (row, 1) the eta basis
+                    // t < 128 the xi basis of target t, thread 128 + t its
+                    // eta basis
                     cur_slot = it.off;
                     producers_sync();
-                    if (rvalid) {
-                        const double2 e = a.xieta[G.tgt + row];
+                    const int brow = tid & (kTcRows - 1);
+                    if (brow < G.nt) {
+                        const double2 e = a.xieta[G.tgt + brow];
                         const double *nodes = a.tgt_nodes + (size_t)it.off * 2 * n;
-                        if (ks == 0) down_basis(e.x, nodes, n, sm.fx[row]);
-                        else down_basis(e.y, nodes + n, n, sm.fe[row]);
+                        if (tid < kTcRows) down_basis(e.x, nodes, n, sm.fx[brow]);
+                        else down_basis(e.y, nodes + n, n, sm.fe[brow]);
                     }
                     producers_sync();
                 }
                 const float2 tx2 = f2(tl0 - it.dx), ty2 = f2(tl1 - it.dy), tz2 = f2(tl2 - it.dz);
                 for (int j = 0; j < nst; ++j, ++st) {
-                    wait_slot(st);
-                    const uint32_t slot = st % kKStages;
-                    if (active) {
+                    const uint32_t slot = st % kKStages, kpar = ((st / kKStages) - 1) & 1;
+                    const int nks = (min(kStageK, it.cnt - kStageK * j) + 7) >> 3;   // k-steps of this stage
+                    // the MMAs that last read this slot must be done before
+                    // the first store into it
+                    bool slot_free = st < (uint32_t)kKStages;
+                    if (MODE == 2 && active && kfirst < nks)
+                        wait_bounded(&sm.wfull[st % kWStages], (st / kWStages) & 1, abort, err);
+#pragma unroll 1
+                    for (int kk = kfirst; active && kk < nks; kk += kstride) {
+                        if (MODE != 2 && kind != 2) {
+                            const float4 *want = kptr(it, j, kk);
+                            if (want != pre_src) fetch(want);   // not prefetched: load now
+                        }
                         float ve[8], vn[8], vz[8];
                         if (MODE == 2) {
                             // upward: the BLI basis of proxy (i, j) at the 8 points,
                             // F_i(xi) G_j(eta) from the per-point factors
-                            wait_bounded(&sm.wfull[st % kWStages], (st / kWStages) & 1, abort, err);
-                            const float *Fb = sm.aux[st % kWStages] + 16 * n * ks;
+                            const float *Fb = sm.aux[st % kWStages] + 16 * n * kk;
                             const float4 f0 = *reinterpret_cast<const float4 *>(Fb + 8 * up_i);
                             const float4 f1 = *reinterpret_cast<const float4 *>(Fb + 8 * up_i + 4);
                             const float4 g0 = *reinterpret_cast<const float4 *>(Fb + 8 * n + 8 * up_j);
@@ -450,7 +492,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(TcArgs a, int *err
                         } else if (MODE == 0 && kind == 2) {
                             // DOWN: BLI basis of the target x its unit vector's
                             // component of the Cartesian row
-                            const int *km0 = sm.kmap + it.row0 + kStageK * j + 8 * ks;
+                            const int *km0 = sm.kmap + it.row0 + kStageK * j + 8 * kk;
                             const float *fxr = sm.fx[row], *fer = sm.fe[row];
 #pragma unroll
                             for (int c = 0; c < 8; ++c) {
@@ -463,13 +505,13 @@ __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(TcArgs a, int *err
                         } else {
                             // PP / PC: kernel value x projected displacement,
                             // two columns per packed instruction
-                            wait_bounded(&sm.wfull[st % kWStages], (st / kWStages) & 1, abort, err);
-                            const float *L = sm.aux[st % kWStages] + 24 * ks;
 #pragma unroll
                             for (int c2 = 0; c2 < 4; ++c2) {
-                                const float2 dx = sub2(*reinterpret_cast<const float2 *>(L + 2 * c2), tx2);
-                                const float2 dy = sub2(*reinterpret_cast<const float2 *>(L + 8 + 2 * c2), ty2);
-                                const float2 dz = sub2(*reinterpret_cast<const float2 *>(L + 16 + 2 * c2), tz2);
+                                // pre[0..1] = x[8], pre[2..3] = y[8], pre[4..5] = z[8]
+                                const float4 X = pre[c2 >> 1], Y = pre[2 + (c2 >> 1)], Z = pre[4 + (c2 >> 1)];
+                                const float2 dx = sub2((c2 & 1) ? make_float2(X.z, X.w) : make_float2(X.x, X.y), tx2);
+                                const float2 dy = sub2((c2 & 1) ? make_float2(Y.z, Y.w) : make_float2(Y.x, Y.y), ty2);
+                                const float2 dz = sub2((c2 & 1) ? make_float2(Z.z, Z.w) : make_float2(Z.x, Z.y), tz2);
                                 float2 mp = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
                                 // mp = 0 only for a source on the target itself (or a
                                 // repeated point): the clamp keeps the value finite
@@ -500,15 +542,27 @@ __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(TcArgs a, int *err
                                 }
                             }
                             // the target itself among these 8 sources: the self pair
-                            const int cs = my_pos - (it.off + kStageK * j + 8 * ks);
+                            const int cs = my_pos - (it.off + kStageK * j + 8 * kk);
                             if (MODE == 0 && kind == 0 && (unsigned)cs < 8u) {
 #pragma unroll
                                 for (int c = 0; c < 8; ++c)
                                     if (c == cs) { ve[c] = self_e; vn[c] = self_n; }
                             }
                         }
+                        // the next task's coordinates: its next k-step in this
+                        // stage, else its first of the next stage or item
+                        // (issued once this task's are consumed)
+                        if (MODE != 2)
+                            fetch(kk + kstride < nks ? kptr(it, j, kk + kstride)
+                                  : j + 1 < nst      ? kptr(it, j + 1, kfirst)
+                                  : k + 1 < ni       ? kptr(nxt, 0, kfirst)
+                                                     : nullptr);
+                        if (!slot_free) {
+                            wait_bounded(&sm.kempty[slot], kpar, abort, err);
+                            slot_free = true;
+                        }
                         // TF32 hi + lo (the tensor cores read lo's top 11 bits)
-                        float *th = sm.Kt[slot][ks][0], *tlo = sm.Kt[slot][ks][1];
+                        float *th = sm.Kt[slot][kk][0], *tlo = sm.Kt[slot][kk][1];
 #pragma unroll
                         for (int hh = 0; hh < 2; ++hh) {
                             const float4 eh = make_float4(tf32_hi(ve[4 * hh]), tf32_hi(ve[4 * hh + 1]),
@@ -538,6 +592,12 @@ __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(TcArgs a, int *err
                                 }
                             }
                         }
+                    }
+                    if (!slot_free) {
+                        // warps that wrote nothing: their arrival must still
+                        // not run a ring phase ahead of the MMAs
+                        wait_bounded(&sm.kempty[slot], kpar, abort, err);
+                    } else {
                         dev::fence_proxy_async();
                     }
                     __syncwarp();
@@ -560,18 +620,18 @@ __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(TcArgs a, int *err
                     const uint32_t slot = st % kKStages, jb = st % kWStages;
                     wait_bounded(&sm.wfull[jb], (st / kWStages) & 1, abort, err);
                     wait_bounded(&sm.kfull[slot], (st / kKStages) & 1, abort, err);
-                    // a new chain reuses the accumulator of chain cc - 2, which must be folded
-                    if (!chain_open && cc >= 2) wait_bounded(&sm.accfree[cc & 1], ((cc >> 1) - 1) & 1, abort, err);
+                    // a new chain overwrites the accumulator, whose last chain
+                    // (cc - 1) the fold warps must have read
+                    if (!chain_open && cc >= 1) wait_bounded(&sm.accfree, (cc - 1) & 1, abort, err);
                     tc_fence_after();
                     if (lane == 0) {
                         if (!*abort) {
-                            const int nks = it.cnt - kStageK * j > 8 ? 2 : 1;
+                            const int nks = (min(kStageK, it.cnt - kStageK * j) + 7) >> 3;
                             for (int s = 0; s < nks; ++s) {
                                 const uint64_t aw = smem_desc(&sm.Wt[jb][s * kWStepFloats]);
                                 const uint64_t bh = smem_desc(sm.Kt[slot][s][0]), bl = smem_desc(sm.Kt[slot][s][1]);
-                                const uint32_t d = tmem + 256 * (cc & 1);
-                                mma_ss(d, aw, bh, (chain_open || s > 0) ? 1u : 0u);
-                                mma_ss(d, aw, bl, 1u);
+                                mma_ss(tmem, aw, bh, (chain_open || s > 0) ? 1u : 0u);
+                                mma_ss(tmem, aw, bl, 1u);
                             }
                         }
                         mma_commit(&sm.kempty[slot]);
@@ -581,7 +641,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(TcArgs a, int *err
                     __syncwarp();
                 }
                 if (it.kind & kTcFlush) {
-                    if (lane == 0) mma_commit(&sm.accfull[cc & 1]);
+                    if (lane == 0) mma_commit(&sm.accfull);
                     __syncwarp();
                     chain_open = false;
                     ++cc;
@@ -609,16 +669,16 @@ __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(TcArgs a, int *err
                     if (lane == 0) {
                         const int ncol = min(kStageK, it.cnt - kStageK * j), nks = (ncol + 7) >> 3;
                         const uint32_t wbytes = (uint32_t)nks * kWStepFloats * 4;
-                        const uint32_t lbytes = MODE == 2 ? (uint32_t)nks * 64 * n
-                                                : ((it.kind & 3) != 2 ? (uint32_t)nks * 96 : 0u);
+                        // upward: the stage's BLI factors come with the weights
+                        // (the other passes' producers read source coordinates
+                        // themselves)
+                        const uint32_t lbytes = MODE == 2 ? (uint32_t)nks * 64 * n : 0u;
                         dev::mbar_expect_tx(&sm.wfull[jb], wbytes + lbytes);
                         if (!*abort) {
-                            if (lbytes) {
-                                const float *src = MODE == 2 ? a.basis + (size_t)(it.row0 + 2 * j) * 16 * n
-                                                             : a.sxyz + (size_t)(it.kb + 2 * j) * 24;
-                                dev::bulk_g2s(sm.aux[jb], src, lbytes, &sm.wfull[jb]);
-                            }
-                            dev::bulk_g2s(sm.Wt[jb], a.bstore + (size_t)(it.kb + 2 * j) * kWStepFloats, wbytes,
+                            if (lbytes)
+                                dev::bulk_g2s(sm.aux[jb], a.basis + (size_t)(it.row0 + kStageKs * j) * 16 * n, lbytes,
+                                              &sm.wfull[jb]);
+                            dev::bulk_g2s(sm.Wt[jb], a.bstore + (size_t)(it.kb + kStageKs * j) * kWStepFloats, wbytes,
                                           &sm.wfull[jb]);
                         }
                     }
@@ -644,16 +704,16 @@ __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(TcArgs a, int *err
             bool first = true;
             for (int k = G.ib; k < G.ie; ++k) {
                 if (!(a.items[k].kind & kTcFlush)) continue;
-                wait_bounded(&sm.accfull[cc & 1], (cc >> 1) & 1, abort, err);
+                wait_bounded(&sm.accfull, cc & 1, abort, err);
                 tc_fence_after();
-                fold_chain<MODE>(tq + 256 * (cc & 1), &sm.run[0][0], q, lane, k == G.ie - 1, first, G.tgt, G.nt,
+                fold_chain<MODE>(tq, q, lane, k == G.ie - 1, first, G.tgt, G.nt,
                                  a.perm, a.out_x, a.out_y, a.ld_out, a.f0, a.nf, *abort != 0,
                                  MODE == 1   ? a.partial + ((size_t)G.out * P + G.row0) * 3 * kF
                                  : MODE == 2 ? a.partial + ((size_t)G.out * P + G.row0) * kF
                                              : nullptr);
                 tc_fence_before();
                 __syncwarp();
-                if (lane == 0) mbar_arrive(&sm.accfree[cc & 1]);
+                if (lane == 0) mbar_arrive(&sm.accfree);
                 first = false;
                 ++cc;
             }
