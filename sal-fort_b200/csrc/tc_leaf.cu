@@ -6,10 +6,10 @@
 // items, and the group's end written to its unit's partial rows.  The leaf
 // pass is described below.
 //
-// One CTA per SM at a time, each walking a few leaf groups of up to 128
-// targets in pool order with a stride of the grid size.  A group's work is a list of
+// One CTA per SM at a time, each walking leaf groups of up to 128 targets
+// in pool order with a stride of the grid size.  A group's work is a list of
 // items (<= 64 sources, or <= 64 Cartesian rows of a DOWN interpolation), cut
-// into stages of 16 K columns (two k-steps of 8).  The contraction is
+// into stages of 32 K columns (four k-steps of 8).  The contraction is
 //     D[field part, target component] += W[field part, k] * T[k, target component]
 // with M = 128 weight rows (64 fields, TF32 hi and lo parts, ordered so that
 // field f's hi row 32(f/16) + f%16 and lo row +16 share a warp) and N = 256
@@ -18,31 +18,33 @@
 // width: per k-step two MMAs, W * T_hi and W * T_lo, give all four hi/lo
 // cross products.
 // Warp roles:
-//   warps 0-7   producers.  Thread t forms target row t % 128 of k-step t / 128
-//               of every stage: 8 kernel-tile entries per component in FP32,
-//               split into TF32 hi + lo, stored to shared memory in the
-//               canonical K-major layout (the MMA's B operand).  The self
-//               pair enters as the tile's diagonal entry: the reference
-//               kernel's FP64 value at distance zero (rounding noise).  The
-//               sources' FP32 coordinates (per k-step x[8] y[8] z[8]) are
-//               read from global memory into registers a stage ahead: a
-//               stage is bound by the latency of its shared-memory round
-//               trips (barrier polls, loads, the proxy fence), not by its
-//               arithmetic, so each one taken off the chain counts.
+//   warps 0-7   producers.  A task is one k-step of a 32-target row block:
+//               8 kernel-tile entries per component and row in FP32, split
+//               into TF32 hi + lo, stored to shared memory in the canonical
+//               K-major layout (the MMA's B operand).  A stage's tasks are
+//               dealt so that small groups use every warp (see the producer
+//               branch).  The self pair enters as the tile's diagonal entry:
+//               the reference kernel's FP64 value at distance zero (rounding
+//               noise).  The sources' FP32 coordinates (per k-step x[8] y[8]
+//               z[8]) are read from global memory into registers a task
+//               ahead.  A stage costs the latency of the busiest warp's tasks
+//               (dependent arithmetic and shared-memory round trips), not
+//               their issue: more warps on fewer tasks each is what helps.
 //   warp 8      issues the MMAs.
 //   warp 9      loads, per stage, the weight tiles (pre-split TF32 hi / lo,
 //               written once per solve by split_store_kernel), and for the
-//               upward pass the BLI factors, with bulk copies into a 4-deep
+//               upward pass the BLI factors, with bulk copies into a 3-deep
 //               ring.
 //   warps 10-13 fold finished accumulator chains into the running sums and
 //               write the outputs (warp w: tensor memory lanes 32(w%4)..+31).
 // The tensor cores accumulate with truncation, so one chain over all of a
 // target's sources would bias the result toward zero: a chain ends after about
-// 32 k-steps (plan flag kTcFlush); its hi and lo rows are added and folded into
-// the group's running sums (shared memory, FP32, round to nearest).  Two
-// accumulators in tensor memory (columns 0-255 and 256-511) alternate between
-// chains, so the tensor cores go on with the next chain while the fold warps
-// fold the last one.
+// 32 k-steps (plan flag kTcFlush) and is folded into the group's running sums
+// with round-to-nearest FP32 adds.  The running sums live in tensor memory
+// (columns 256-511, the accumulator's row layout) next to the accumulator
+// (columns 0-255); shared memory holds only the operand rings.  The next chain
+// starts once the fold warps have read the accumulator; the two-stage
+// kernel-tile ring lets the producers run on meanwhile.
 #include <cuda_runtime.h>
 
 #include "kernels.cuh"
