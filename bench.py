@@ -364,8 +364,8 @@ def main():
                 "flops_counted": "algorithmic 4*F per pair (2 components x FMA x F fields); the hi/lo split "
                                  "executes 4x these on the tensor cores (W_hi,W_lo x T_hi,T_lo), plus padding",
                 # ncu dram__bytes_read.sum + dram__bytes_write.sum of one tc_leaf_kernel launch on the
-                # 655,362-cell, 64-field case (3.53 + 2.62 GB), scaled by the cell count
-                "traffic": 6.156e9 * g.n / 655362 if F == 64 else None,
+                # 655,362-cell, 64-field case (3.55 + 2.63 GB), scaled by the cell count
+                "traffic": 6.180e9 * g.n / 655362 if F == 64 else None,
                 "traffic_source": "ncu capture on 655,362 cells x 64 fields, scaled by cells",
                 "leaf_ms": leaf_ms, "proxy_ms": proxy_ms, "prep_upward_ms": up_ms}
     else:
