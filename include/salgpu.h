@@ -162,6 +162,22 @@ int sal_solve(sal_grid *g, const double *ssh, int32_t nfields, int64_t ld_ssh, d
 int sal_solve_host(sal_grid *g, const double *ssh, int32_t nfields, int64_t ld_ssh, double *out_x, double *out_y,
                    int64_t ld_out, int32_t form);
 
+/* Pipelined sal_solve_host.  No counterpart in the reference: it serves callers
+ * that solve one batch after another from host memory.  The call enqueues the
+ * copy of the fields to the device, the solve and the copy of both components
+ * back, and returns without waiting.  The grid alternates two device staging
+ * slots and copies on two streams of its own.  So one call's copies overlap the
+ * neighbouring calls' solves, and its copy back overlaps the next copy in.
+ * Host buffers must be pinned (cudaHostAlloc or cudaHostRegister) for the
+ * copies to be asynchronous.  They must stay valid and unmodified until
+ * sal_solve_host_wait returns.  Arguments and results as in sal_solve_host. */
+int sal_solve_host_async(sal_grid *g, const double *ssh, int32_t nfields, int64_t ld_ssh, double *out_x,
+                         double *out_y, int64_t ld_out, int32_t form);
+
+/* Waits for every sal_solve_host_async call on the grid; reports a device-side
+ * error of any of them (SAL_ETIMEOUT, ...). */
+int sal_solve_host_wait(sal_grid *g);
+
 /* fast_sum, fast_sum_module.f90:291-332: adds the SAL gradient of one field
  * into host arrays sal_longrad/sal_latgrad (intent(inout)).  The grid must be
  * SAL_MODE_DTT.  form as in sal_solve. */

@@ -83,6 +83,15 @@ struct GridImpl {
     double *h_ssh = nullptr, *h_ox = nullptr, *h_oy = nullptr;  // device
     double *hb_ssh = nullptr, *hb_ox = nullptr, *hb_oy = nullptr;  // device, batched
     int hb_fields = 0;
+    // pipelined host solves: two device staging slots, copy streams of their own
+    struct HostSlot {
+        double *ssh = nullptr, *ox = nullptr, *oy = nullptr;
+        int64_t fields = 0;
+        cudaEvent_t in = nullptr, solved = nullptr, out = nullptr;
+        bool used = false;
+    } hslot[2];
+    int hnext = 0;
+    cudaStream_t s_in = nullptr, s_out = nullptr;
     double *h_w = nullptr;                                        // device, P*npanels
     std::vector<void *> allocs;
     std::mutex mu;
@@ -134,6 +143,11 @@ static void grid_free(GridImpl &g) {
     if (g.dev >= 0) cudaSetDevice(g.dev);
     for (auto &e : g.ev)
         if (e) cudaEventDestroy(e);
+    for (auto &h : g.hslot)
+        for (cudaEvent_t e : {h.in, h.solved, h.out})
+            if (e) cudaEventDestroy(e);
+    if (g.s_in) cudaStreamDestroy(g.s_in);
+    if (g.s_out) cudaStreamDestroy(g.s_out);
     for (void *p : g.allocs) cudaFree(p);
     g.allocs.clear();
     if (g.stream) cudaStreamDestroy(g.stream);
@@ -676,6 +690,64 @@ extern "C" int sal_solve_host(sal_grid *G, const double *ssh, int32_t nf, int64_
         CK(cudaMemcpyAsync(oy + (size_t)f * ld_out, g.hb_oy + (size_t)f * n, (size_t)n * 8, cudaMemcpyDeviceToHost,
                            g.stream));
     }
+    return finish(g, g.stream);
+}
+
+// Slot k's buffers are reused two calls later: its copy in waits for the solve
+// that read its fields, and its solve waits for the copy out of its results.
+extern "C" int sal_solve_host_async(sal_grid *G, const double *ssh, int32_t nf, int64_t ld_ssh, double *ox, double *oy,
+                                    int64_t ld_out, int32_t form) {
+    if (!G || !ssh || !ox || !oy) return set_error(SAL_EINVAL, "null argument");
+    GridImpl &g = G->g;
+    const int64_t n = g.plan.n;
+    if (nf < 1) return set_error(SAL_EINVAL, "nfields must be >= 1");
+    if (nf > 1 && (ld_ssh < n || ld_out < n)) return set_error(SAL_EINVAL, "leading dimension < point_count");
+    std::lock_guard<std::mutex> lk(g.mu);
+    CK(cudaSetDevice(g.dev));
+    if (!g.s_in) {
+        CK(cudaStreamCreateWithFlags(&g.s_in, cudaStreamNonBlocking));
+        CK(cudaStreamCreateWithFlags(&g.s_out, cudaStreamNonBlocking));
+        for (auto &h : g.hslot)
+            for (cudaEvent_t *e : {&h.in, &h.solved, &h.out}) CK(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+    }
+    GridImpl::HostSlot &h = g.hslot[g.hnext];
+    g.hnext ^= 1;
+    if (h.fields < nf) {
+        if (h.used) CK(cudaEventSynchronize(h.out));
+        int rc = dalloc(g, &h.ssh, (size_t)n * nf);
+        if (!rc) rc = dalloc(g, &h.ox, (size_t)n * nf);
+        if (!rc) rc = dalloc(g, &h.oy, (size_t)n * nf);
+        if (rc) return rc;
+        h.fields = nf;
+    }
+    if (h.used) CK(cudaStreamWaitEvent(g.s_in, h.solved, 0));
+    for (int f = 0; f < nf; ++f)
+        CK(cudaMemcpyAsync(h.ssh + (size_t)f * n, ssh + (size_t)f * ld_ssh, (size_t)n * 8, cudaMemcpyHostToDevice,
+                           g.s_in));
+    CK(cudaEventRecord(h.in, g.s_in));
+    CK(cudaStreamWaitEvent(g.stream, h.in, 0));
+    if (h.used) CK(cudaStreamWaitEvent(g.stream, h.out, 0));
+    int rc = sal_solve(G, h.ssh, nf, n, h.ox, h.oy, n, form, g.stream);
+    if (rc) return rc;
+    CK(cudaEventRecord(h.solved, g.stream));
+    CK(cudaStreamWaitEvent(g.s_out, h.solved, 0));
+    for (int f = 0; f < nf; ++f) {
+        CK(cudaMemcpyAsync(ox + (size_t)f * ld_out, h.ox + (size_t)f * n, (size_t)n * 8, cudaMemcpyDeviceToHost,
+                           g.s_out));
+        CK(cudaMemcpyAsync(oy + (size_t)f * ld_out, h.oy + (size_t)f * n, (size_t)n * 8, cudaMemcpyDeviceToHost,
+                           g.s_out));
+    }
+    CK(cudaEventRecord(h.out, g.s_out));
+    h.used = true;
+    return SAL_OK;
+}
+
+extern "C" int sal_solve_host_wait(sal_grid *G) {
+    if (!G) return set_error(SAL_EINVAL, "null argument");
+    GridImpl &g = G->g;
+    std::lock_guard<std::mutex> lk(g.mu);
+    CK(cudaSetDevice(g.dev));
+    if (g.s_out) CK(cudaStreamSynchronize(g.s_out));
     return finish(g, g.stream);
 }
 

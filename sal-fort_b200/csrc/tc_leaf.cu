@@ -464,6 +464,9 @@ __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(TcArgs a, int *err
                     producers_sync();
                 }
                 const float2 tx2 = f2(tl0 - it.dx), ty2 = f2(tl1 - it.dy), tz2 = f2(tl2 - it.dz);
+                // only the item whose sources are the group's own points holds
+                // self pairs (one test per item, the same for every thread)
+                const bool self_item = MODE == 0 && kind == 0 && it.off < G.tgt + G.nt && G.tgt < it.off + it.cnt;
                 for (int j = 0; j < nst; ++j, ++st) {
                     const uint32_t slot = st % kKStages, kpar = ((st / kKStages) - 1) & 1;
                     const int nks = (min(kStageK, it.cnt - kStageK * j) + 7) >> 3;   // k-steps of this stage
@@ -544,11 +547,13 @@ __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(TcArgs a, int *err
                                 }
                             }
                             // the target itself among these 8 sources: the self pair
-                            const int cs = my_pos - (it.off + kStageK * j + 8 * kk);
-                            if (MODE == 0 && kind == 0 && (unsigned)cs < 8u) {
+                            if (self_item) {
+                                const int cs = my_pos - (it.off + kStageK * j + 8 * kk);
+                                if ((unsigned)cs < 8u) {
 #pragma unroll
-                                for (int c = 0; c < 8; ++c)
-                                    if (c == cs) { ve[c] = self_e; vn[c] = self_n; }
+                                    for (int c = 0; c < 8; ++c)
+                                        if (c == cs) { ve[c] = self_e; vn[c] = self_n; }
+                                }
                             }
                         }
                         // the next task's coordinates: its next k-step in this

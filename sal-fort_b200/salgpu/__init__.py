@@ -36,7 +36,8 @@ EXPORTS = (
     "sal_tree_destroy", "sal_dual_tree_traversal", "sal_single_tree_traversal", "sal_assign_points_to_panels",
     "sal_grid_create", "sal_grid_stats_get", "sal_grid_sync", "sal_grid_destroy", "sal_solve", "sal_fast_sum_host",
     "sal_proxy_source_compute_host", "sal_pc_compute_host", "sal_pp_compute_host", "sal_direct_sum",
-    "sal_grid_timing", "sal_fma_peak", "sal_direct_sum_noalloc", "sal_solve_host",
+    "sal_grid_timing", "sal_fma_peak", "sal_direct_sum_noalloc", "sal_solve_host", "sal_solve_host_async",
+    "sal_solve_host_wait",
 )
 
 
@@ -104,6 +105,8 @@ def lib():
         L.sal_solve.argtypes = [vp, vp, i32, i64, vp, vp, i64, i32, vp]
         L.sal_fast_sum_host.argtypes = [vp, vp, vp, vp, i32]
         L.sal_solve_host.argtypes = [vp, vp, i32, i64, vp, vp, i64, i32]
+        L.sal_solve_host_async.argtypes = [vp, vp, i32, i64, vp, vp, i64, i32]
+        L.sal_solve_host_wait.argtypes = [vp]
         L.sal_proxy_source_compute_host.argtypes = [vp, vp, vp]
         L.sal_pc_compute_host.argtypes = [vp, vp, vp, vp]
         L.sal_pp_compute_host.argtypes = [vp, vp, vp, vp]
@@ -313,6 +316,19 @@ class Grid:
         outputs overwritten.  Pinned arrays make the copies asynchronous."""
         F = ssh.shape[0] if ssh.ndim == 2 else 1
         _check(lib().sal_solve_host(self.handle, _ptr(ssh), F, self.n, _ptr(out_x), _ptr(out_y), self.n, int(form)))
+
+    def solve_host_async(self, ssh, out_x, out_y, form=FORM_REF):
+        """Pipelined solve on host arrays (sal_solve_host_async): enqueues the
+        copies and the solve and returns.  The arrays must be pinned (for
+        example numpy views of pinned torch tensors) and left untouched until
+        solve_host_wait() returns."""
+        F = ssh.shape[0] if ssh.ndim == 2 else 1
+        _check(lib().sal_solve_host_async(self.handle, _ptr(ssh), F, self.n, _ptr(out_x), _ptr(out_y), self.n,
+                                          int(form)))
+
+    def solve_host_wait(self):
+        """Waits for every solve_host_async call of this grid."""
+        _check(lib().sal_solve_host_wait(self.handle))
 
     # ---- host-buffer entry points (synchronous, add into the outputs)
     def fast_sum_host(self, ssh, sal_longrad, sal_latgrad, form=FORM_REF):

@@ -106,3 +106,25 @@ def test_tcgen05_passes_at_other_degrees(degree):
     assert not (torch.isnan(mx).any() or torch.isnan(my).any())
     for f in range(3):
         assert rel_l2(mx[f].cpu().numpy(), my[f].cpu().numpy(), ax[f].cpu().numpy(), ay[f].cpu().numpy()) <= 5e-6
+
+
+def test_host_entry_points_and_pipelined_calls_match_device_solve():
+    """sal_solve_host and three pipelined sal_solve_host_async calls (two
+    staging slots, inputs alternating) give the device solve's results bit for
+    bit; the second input has its fields reversed, so its results come back
+    reversed."""
+    torch = _torch()
+    S, g, hs, grid = _grid("small_3000", 20, 64, seed=5)
+    dx, dy = grid.solve(torch.tensor(hs, device="cuda"), form=S.FORM_MIXED)
+    dx, dy = dx.cpu(), dy.cpu()
+    h_in = [torch.tensor(hs).pin_memory(), torch.tensor(hs[::-1].copy()).pin_memory()]
+    outs = [(torch.empty_like(h_in[0]).pin_memory(), torch.empty_like(h_in[0]).pin_memory()) for _ in range(3)]
+    for k in range(3):
+        grid.solve_host_async(h_in[k % 2].numpy(), outs[k][0].numpy(), outs[k][1].numpy(), S.FORM_MIXED)
+    grid.solve_host_wait()
+    sx, sy = torch.empty_like(h_in[0]).pin_memory(), torch.empty_like(h_in[0]).pin_memory()
+    grid.solve_host(h_in[0].numpy(), sx.numpy(), sy.numpy(), S.FORM_MIXED)
+    assert torch.equal(sx, dx) and torch.equal(sy, dy)
+    for k in (0, 2):
+        assert torch.equal(outs[k][0], dx) and torch.equal(outs[k][1], dy)
+    assert torch.equal(outs[1][0], dx.flip(0)) and torch.equal(outs[1][1], dy.flip(0))
