@@ -142,6 +142,15 @@ int sal_grid_sync(sal_grid *g, void *stream);
  * number of solves summed. */
 int sal_grid_timing(sal_grid *g, int32_t enable, double *phase_ms, int64_t *solves);
 
+/* CUDA graphs of batched solves.  enable = 1: the first SAL_FORM_MIXED
+ * sal_solve of each call shape (field and output pointers, nfields, leading
+ * dimensions) on a non-NULL stream runs as usual and is then captured into a
+ * graph, on a stream of the caller stream's priority; later solves of that
+ * shape launch the graph on their stream.  The grid keeps up to 128 graphs,
+ * dropping the oldest.  0 frees them and solves launch kernel by kernel again.
+ * Graphs are not used while the per-pass timers are on. */
+int sal_grid_set_graphs(sal_grid *g, int32_t enable);
+
 /* Throughput of the FP64 (precision 64) or FP32 (precision 32) fused
  * multiply-add pipe of the current device, measured by a dependent-chain
  * microbenchmark: *tflops receives the achieved TFLOP/s (2 flops per FMA). */

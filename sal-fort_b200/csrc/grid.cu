@@ -92,6 +92,23 @@ struct GridImpl {
     } hslot[2];
     int hnext = 0;
     cudaStream_t s_in = nullptr, s_out = nullptr;
+    // CUDA graphs of batched solves, one per call shape (sal_grid_set_graphs)
+    struct GraphShape {
+        const double *ssh;
+        int32_t nf;
+        int64_t ld_ssh;
+        double *ox, *oy;
+        int64_t ld_out;
+        bool operator==(const GraphShape &o) const {
+            return ssh == o.ssh && nf == o.nf && ld_ssh == o.ld_ssh && ox == o.ox && oy == o.oy && ld_out == o.ld_out;
+        }
+    };
+    struct GraphEntry {
+        GraphShape shape;
+        cudaGraphExec_t exec;
+    };
+    bool use_graphs = false;
+    std::vector<GraphEntry> graphs;
     double *h_w = nullptr;                                        // device, P*npanels
     std::vector<void *> allocs;
     std::mutex mu;
@@ -146,6 +163,8 @@ static void grid_free(GridImpl &g) {
     for (auto &h : g.hslot)
         for (cudaEvent_t e : {h.in, h.solved, h.out})
             if (e) cudaEventDestroy(e);
+    for (auto &e : g.graphs) cudaGraphExecDestroy(e.exec);
+    g.graphs.clear();
     if (g.s_in) cudaStreamDestroy(g.s_in);
     if (g.s_out) cudaStreamDestroy(g.s_out);
     for (void *p : g.allocs) cudaFree(p);
@@ -574,6 +593,48 @@ static void solve_mixed_block(GridImpl &g, const double *ssh, int64_t ld_ssh, in
     }
 }
 
+// Captures the batched solve of one call shape into a graph (nothing runs).
+// The capture stream takes the caller stream's priority, which the graph's
+// kernels keep.  Every allocation and kernel attribute the solve needs exists
+// already: the same shape has just run.
+static int capture_mixed(GridImpl &g, const GridImpl::GraphShape &k, cudaStream_t caller) {
+    constexpr size_t kMaxGraphs = 128;
+    int prio = 0;
+    CK(cudaStreamGetPriority(caller, &prio));
+    cudaStream_t cs = nullptr;
+    CK(cudaStreamCreateWithPriority(&cs, cudaStreamNonBlocking, prio));
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+        for (int f0 = 0; f0 < k.nf; f0 += g.FT) solve_mixed_block(g, k.ssh, k.ld_ssh, f0, k.nf, k.ox, k.oy, k.ld_out, cs);
+        e = cudaStreamEndCapture(cs, &graph);
+    }
+    cudaGraphExec_t exec = nullptr;
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
+    if (graph) cudaGraphDestroy(graph);
+    cudaStreamDestroy(cs);
+    if (e != cudaSuccess) return set_error(SAL_ECUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+    if (g.graphs.size() >= kMaxGraphs) {
+        cudaGraphExecDestroy(g.graphs.front().exec);
+        g.graphs.erase(g.graphs.begin());
+    }
+    g.graphs.push_back({k, exec});
+    return SAL_OK;
+}
+
+extern "C" int sal_grid_set_graphs(sal_grid *G, int32_t enable) {
+    if (!G) return set_error(SAL_EINVAL, "null argument");
+    GridImpl &g = G->g;
+    std::lock_guard<std::mutex> lk(g.mu);
+    CK(cudaSetDevice(g.dev));
+    if (!enable) {
+        for (auto &e : g.graphs) cudaGraphExecDestroy(e.exec);
+        g.graphs.clear();
+    }
+    g.use_graphs = enable != 0;
+    return SAL_OK;
+}
+
 extern "C" int sal_solve(sal_grid *G, const double *ssh, int32_t nf, int64_t ld_ssh, double *ox, double *oy,
                          int64_t ld_out, int32_t form, void *stream) {
     if (!G || !ssh || !ox || !oy) return set_error(SAL_EINVAL, "null argument");
@@ -589,9 +650,17 @@ extern "C" int sal_solve(sal_grid *G, const double *ssh, int32_t nf, int64_t ld_
         const int FT = g.FT ? g.FT : (g.max_fields <= 32 ? 32 : 64);
         int rc = ensure_mixed(g, FT);
         if (rc) return rc;
+        const bool graph = g.use_graphs && st != nullptr && !g.timing;
+        const GridImpl::GraphShape shape{ssh, nf, ld_ssh, ox, oy, ld_out};
+        if (graph)
+            for (const auto &e : g.graphs)
+                if (e.shape == shape) {
+                    CK(cudaGraphLaunch(e.exec, st));
+                    return SAL_OK;
+                }
         for (int f0 = 0; f0 < nf; f0 += FT) solve_mixed_block(g, ssh, ld_ssh, f0, nf, ox, oy, ld_out, st);
         CK(cudaGetLastError());
-        return SAL_OK;
+        return graph ? capture_mixed(g, shape, st) : SAL_OK;
     }
     for (int f = 0; f < nf; ++f)
         solve_fp64(g, ssh + (size_t)f * ld_ssh, ox + (size_t)f * ld_out, oy + (size_t)f * ld_out,

@@ -37,7 +37,7 @@ EXPORTS = (
     "sal_grid_create", "sal_grid_stats_get", "sal_grid_sync", "sal_grid_destroy", "sal_solve", "sal_fast_sum_host",
     "sal_proxy_source_compute_host", "sal_pc_compute_host", "sal_pp_compute_host", "sal_direct_sum",
     "sal_grid_timing", "sal_fma_peak", "sal_direct_sum_noalloc", "sal_solve_host", "sal_solve_host_async",
-    "sal_solve_host_wait",
+    "sal_solve_host_wait", "sal_grid_set_graphs",
 )
 
 
@@ -107,6 +107,7 @@ def lib():
         L.sal_solve_host.argtypes = [vp, vp, i32, i64, vp, vp, i64, i32]
         L.sal_solve_host_async.argtypes = [vp, vp, i32, i64, vp, vp, i64, i32]
         L.sal_solve_host_wait.argtypes = [vp]
+        L.sal_grid_set_graphs.argtypes = [vp, i32]
         L.sal_proxy_source_compute_host.argtypes = [vp, vp, vp]
         L.sal_pc_compute_host.argtypes = [vp, vp, vp, vp]
         L.sal_pp_compute_host.argtypes = [vp, vp, vp, vp]
@@ -316,6 +317,12 @@ class Grid:
         outputs overwritten.  Pinned arrays make the copies asynchronous."""
         F = ssh.shape[0] if ssh.ndim == 2 else 1
         _check(lib().sal_solve_host(self.handle, _ptr(ssh), F, self.n, _ptr(out_x), _ptr(out_y), self.n, int(form)))
+
+    def set_graphs(self, enable=True):
+        """CUDA graphs of batched solves, one per call shape (sal_grid_set_graphs):
+        the first FORM_MIXED solve of a shape on a non-default stream is
+        captured, later ones launch the graph."""
+        _check(lib().sal_grid_set_graphs(self.handle, 1 if enable else 0))
 
     def solve_host_async(self, ssh, out_x, out_y, form=FORM_REF):
         """Pipelined solve on host arrays (sal_solve_host_async): enqueues the
