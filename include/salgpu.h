@@ -142,7 +142,8 @@ int sal_grid_sync(sal_grid *g, void *stream);
  * number of solves summed. */
 int sal_grid_timing(sal_grid *g, int32_t enable, double *phase_ms, int64_t *solves);
 
-/* CUDA graphs of batched solves.  enable = 1: the first SAL_FORM_MIXED
+/* CUDA graphs of batched solves (no counterpart in the reference, which
+ * solves one field per run).  enable = 1: the first SAL_FORM_MIXED
  * sal_solve of each call shape (field and output pointers, nfields, leading
  * dimensions) on a non-NULL stream runs as usual and is then captured into a
  * graph, on a stream of the caller stream's priority; later solves of that
