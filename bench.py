@@ -55,6 +55,7 @@ def _args():
     ap.add_argument("--serve-rate", type=float, default=200.0)
     ap.add_argument("--serve-host", action="store_true", help="serving requests carry host arrays")
     ap.add_argument("--no-serve", action="store_true")
+    ap.add_argument("--cpu-table", action="store_true", help="time the oracle on cfg0/cfg1/cfg2 and exit")
     a = ap.parse_args()
     if a.fields is None:
         a.fields = 64 if a.form == "mixed" else 1
@@ -112,38 +113,62 @@ def make_problem(args, device):
     return g, h, time.perf_counter() - t0
 
 
-def cpu_baseline(args, g, h, sample_seconds):
-    """The oracle (a line-faithful C restatement of the reference) on a random
-    seeded sample of the interaction list with all host threads; the full
-    one-field solve time is extrapolated by the sampled fraction of the list.
-    The reference solves one field per call, so its evals/s is the same for
-    any number of fields."""
+RANK_SPLIT = 8      # the reference's MPI split of the DTT list, MOD(i, P) == rank (fast_sum_module.f90:304)
+
+
+def cpu_shares(args, g):
+    """The oracle's tree and DTT list of the grid, split into the RANK_SPLIT
+    shares MOD(i, P) == r of fast_sum_module.f90:304, each with its fraction of
+    the solve's pair + MAC work."""
     from oracle import oracle as O
-    cores = os.cpu_count() or 1
     t0 = time.perf_counter()
     ot = O.tree_traverse(g.xs, g.ys, g.zs, args.thresh)
     L = O.dual_tree_traversal(ot, args.theta, args.thresh)
     setup = time.perf_counter() - t0
     pairs_all, macs_all = O.dtt_work(ot, L, args.degree)
-    rng = np.random.default_rng(1234)
-    frac = 0.002
-    while True:
-        sel = np.sort(rng.choice(len(L), max(1, int(frac * len(L))), replace=False))
-        t1 = time.perf_counter()
-        O.fast_sum(ot, L[sel], g.xs, g.ys, g.zs, g.areas, h, args.degree, nranks=cores)
-        dt = time.perf_counter() - t1
-        if dt > 0.25 * sample_seconds or frac >= 1.0:
+    i = np.arange(1, len(L) + 1)
+    shares, frac = [], []
+    for r in range(RANK_SPLIT):
+        sh = L[(i % RANK_SPLIT) == r]
+        p, m = O.dtt_work(ot, sh, args.degree)
+        shares.append(sh)
+        frac.append((p.sum() + m) / (pairs_all.sum() + macs_all))
+    return ot, L, shares, frac, setup
+
+
+def solve_share(args, g, h, ot, share, cores):
+    """One rank's share of a one-field solve: the oracle's fast_sum (a
+    line-faithful C restatement of fast_sum_module.f90) over the share with all
+    host threads."""
+    from oracle import oracle as O
+    t1 = time.perf_counter()
+    O.fast_sum(ot, share, g.xs, g.ys, g.zs, g.areas, h, args.degree, nranks=cores)
+    return time.perf_counter() - t1
+
+
+def cpu_baseline(args, g, h, sample_seconds):
+    """The oracle on the host's cores, measured (not extrapolated): rank
+    shares of one field's solve are timed one after another until
+    sample_seconds have passed or all RANK_SPLIT shares (a complete solve) are
+    done.  evals/s = cells x (work fraction of the timed shares) / time.  The
+    reference solves one field per call, so its evals/s is the same for any
+    number of fields."""
+    cores = os.cpu_count() or 1
+    ot, L, shares, frac, setup = cpu_shares(args, g)
+    t, f, done = 0.0, 0.0, 0
+    for r in range(RANK_SPLIT):
+        t += solve_share(args, g, h, ot, shares[r], cores)
+        f += frac[r]
+        done += 1
+        if t >= sample_seconds:
             break
-        frac = min(1.0, frac * max(2.0, 0.5 * sample_seconds / max(dt, 1e-3)))
-    pairs_s, macs_s = O.dtt_work(ot, L[sel], args.degree)
-    f_work = (pairs_s.sum() + macs_s) / (pairs_all.sum() + macs_all)
-    f_list = len(sel) / len(L)
-    t_full = dt / f_list
-    return {"value": g.n / t_full, "unit": "evals/s", "cores": cores, "kind": "port",
-            "sample": f"one field: {len(sel)} of {len(L)} DTT interactions ({100 * f_list:.2f}%, seeded uniform; "
-                      f"{100 * f_work:.2f}% of pair+MAC work), {dt:.1f} s on {cores} threads, "
-                      f"full solve extrapolated to {t_full:.1f} s; host setup {setup:.1f} s",
-            "extrapolated_solve_s": t_full}
+    whole = done == RANK_SPLIT
+    return {"value": g.n * f / t, "unit": "evals/s", "cores": cores, "kind": "port",
+            "sample": (f"one field, {done} of the {RANK_SPLIT} rank shares MOD(i,{RANK_SPLIT})==r of the "
+                       f"{len(L)}-interaction DTT list ({100 * f:.1f}% of the pair+MAC work"
+                       f"{', a complete solve' if whole else ''}), {t:.1f} s measured on {cores} threads; "
+                       f"host tree + list setup {setup:.1f} s"),
+            "solve_s": t / f, "measured_s": t, "complete_solve": whole}
 
 
 def workload_name(args, n):
@@ -155,21 +180,121 @@ def workload_name(args, n):
 
 
 def run_reference(args):
+    """The reference's CPU algorithm (the oracle port; no Fortran compiler
+    exists on these machines) on the host's cores.  One step is one rank's
+    share MOD(i, 8) == r of a one-field solve of the same grid (the reference's
+    own MPI decomposition of the list, fast_sum_module.f90:304), r cycling
+    through the eight shares, solved with every host thread; every step is
+    timed whole.  value = cells x (work fraction of the timed shares) / time."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     args.fields = 1
+    cores = os.cpu_count() or 1
     g, h, _ = make_problem(args, "cuda" if _cuda() else "cpu")
-    cb = cpu_baseline(args, g, h[0], args.cpu_seconds)
-    line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": "evals/s", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * cb["extrapolated_solve_s"],
+    ot, L, shares, frac, setup = cpu_shares(args, g)
+    for k in range(args.warmup):
+        solve_share(args, g, h[0], ot, shares[k % RANK_SPLIT], cores)
+    times, f = [], 0.0
+    for k in range(args.steps):
+        r = k % RANK_SPLIT
+        times.append(solve_share(args, g, h[0], ot, shares[r], cores))
+        f += frac[r]
+    total = float(np.sum(times))
+    value = g.n * f / total
+    cb = {"value": value, "unit": "evals/s", "cores": cores, "kind": "port",
+          "sample": (f"each step one of the {RANK_SPLIT} rank shares MOD(i,{RANK_SPLIT})==r of the "
+                     f"{len(L)}-interaction DTT list of one field (steps cover {f:.2f} complete solves), "
+                     f"oracle fast_sum on {cores} threads; host tree + list setup {setup:.1f} s")}
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "evals/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic: seeded Fibonacci ocean grid + spherical-harmonic SSH",
             "config": {"workload": workload_name(args, g.n) + " (reference algorithm, one field per call)",
-                       "cells": g.n, "fields": 1},
+                       "cells": g.n, "fields": 1, "step": f"one rank share (1/{RANK_SPLIT} of the list)"},
             "cpu_baseline": cb,
-            "e2e": {"value": cb["value"], "unit": "evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "e2e": {"value": value, "unit": "evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def cpu_table(args):
+    """BASELINE.md's CPU table: the reference's algorithms (the oracle port)
+    on the host's cores, setup and solve timed apart, each with its error
+    against the FP64 direct sum (GPU direct sum when a GPU is present, else
+    the oracle's).  Prints one JSON line."""
+    from oracle import oracle as O
+    from salgpu import synth
+    cores = os.cpu_count() or 1
+    rows = []
+
+    def err_vs_direct(g, h, x, y, tg):
+        if _cuda():
+            import torch
+            import salgpu as S
+            T = lambda a: torch.tensor(a, device="cuda")
+            dx, dy = S.direct_sum(T(g.xs), T(g.ys), T(g.zs), T(g.areas * h), T(tg.astype(np.int32)))
+            dx, dy = dx.cpu().numpy(), dy.cpu().numpy()
+        else:
+            dx, dy = O.direct_sum(g.xs, g.ys, g.zs, g.areas, h, tg, cores)
+        ex, ey = x[tg] - dx, y[tg] - dy
+        return (float(np.sqrt(np.sum(ex * ex + ey * ey) / np.sum(dx * dx + dy * dy))),
+                float(np.max(np.hypot(ex, ey)) / np.max(np.hypot(dx, dy))))
+
+    def sample(g, k, seed=99):
+        return np.sort(np.random.default_rng(seed).choice(g.n, min(k, g.n), replace=False))
+
+    # cfg0: DTT (code.f90), 1 thread and all threads
+    g = synth.config_grid("cfg0")
+    h = synth.config_ssh("cfg0", g)[0]
+    t0 = time.perf_counter()
+    ot = O.tree_traverse(g.xs, g.ys, g.zs, 100)
+    L = O.dual_tree_traversal(ot, 0.7, 100)
+    setup = time.perf_counter() - t0
+    for th in (1, cores):
+        t0 = time.perf_counter()
+        x, y = O.fast_sum(ot, L, g.xs, g.ys, g.zs, g.areas, h, 8, nranks=th)
+        dt = time.perf_counter() - t0
+        e, m = err_vs_direct(g, h, x, y, np.arange(g.n))
+        rows.append({"config": "cfg0", "path": "DTT fast_sum", "cells": g.n, "threads": th, "setup_s": setup,
+                     "solve_s": dt, "evals_per_s": g.n / dt, "rel_l2_vs_direct": e, "max_over_max": m,
+                     "targets": g.n})
+    # cfg1: STT (mom6_code.f90), both proxy-weight orientations, all threads
+    g = synth.config_grid("cfg1")
+    h = synth.config_ssh("cfg1", g, seed=13)[0]
+    t0 = time.perf_counter()
+    ot = O.tree_traverse(g.xs, g.ys, g.zs, 200)
+    ppan = O.assign_points_to_panels(ot, g.xs, g.ys, g.zs)
+    pc, pp = O.single_tree_traversal(ot, 0.7, 200, g.xs, g.ys, g.zs)
+    setup = time.perf_counter() - t0
+    for tr in (True, False):
+        t0 = time.perf_counter()
+        w = O.proxy_source_compute(ot, ppan, g.xs, g.ys, g.zs, h, g.areas, 8, tr, nthreads=cores)
+        t1 = time.perf_counter()
+        x, y = O.pc_compute(ot, pc, g.xs, g.ys, g.zs, 8, w, nthreads=cores)
+        t2 = time.perf_counter()
+        O.pp_compute(ot, pp, g.xs, g.ys, g.zs, g.areas, h, out=(x, y), nthreads=cores)
+        t3 = time.perf_counter()
+        e, m = err_vs_direct(g, h, x, y, sample(g, 10000))
+        rows.append({"config": "cfg1", "path": "STT mom6 " + ("ref_compat (transposed weights)" if tr else "correct"),
+                     "cells": g.n, "threads": cores, "setup_s": setup, "solve_s": t3 - t0,
+                     "phases_s": {"proxy_source_compute": t1 - t0, "pc_compute": t2 - t1, "pp_compute": t3 - t2},
+                     "evals_per_s": g.n / (t3 - t0), "rel_l2_vs_direct": e, "max_over_max": m, "targets": 10000,
+                     "pc_entries": len(pc), "pp_entries": len(pp)})
+    # cfg2: DTT, all threads, a complete solve
+    g = synth.config_grid("cfg2")
+    h = synth.config_ssh("cfg2", g, seed=17)[0]
+    t0 = time.perf_counter()
+    ot = O.tree_traverse(g.xs, g.ys, g.zs, 200)
+    L = O.dual_tree_traversal(ot, 0.7, 200)
+    setup = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    x, y = O.fast_sum(ot, L, g.xs, g.ys, g.zs, g.areas, h, 8, nranks=cores)
+    dt = time.perf_counter() - t0
+    e, m = err_vs_direct(g, h, x, y, sample(g, 10000))
+    rows.append({"config": "cfg2", "path": "DTT fast_sum", "cells": g.n, "threads": cores, "setup_s": setup,
+                 "solve_s": dt, "evals_per_s": g.n / dt, "rel_l2_vs_direct": e, "max_over_max": m,
+                 "targets": 10000})
+    print(json.dumps({"cpu_table": rows, "kind": "port", "cores": cores}), flush=True)
 
 
 def serving_run(args, S, torch, dev):
@@ -249,6 +374,8 @@ def time_solves(torch, grid, ssh, form, out, steps, flush, stream):
 
 def main():
     args = _args()
+    if args.cpu_table:
+        return cpu_table(args)
     if args.impl == "reference":
         return run_reference(args)
     import torch
@@ -323,7 +450,7 @@ def main():
         mxs.append(float(torch.sqrt(ex * ex + ey * ey).max() / torch.sqrt(dx * dx + dy * dy).max()))
 
     # ---- plain FP64 form of the same grid, for the batched-vs-plain ratio
-    plain = None
+    plain = plain_e2e = None
     if form == S.FORM_MIXED and not args.no_fp64:
         s1 = ssh[:1].contiguous()
         o1 = (torch.empty_like(s1), torch.empty_like(s1))
@@ -331,6 +458,15 @@ def main():
             grid.solve(s1, form=S.FORM_REF, out=o1)
         pp = time_solves(torch, grid, s1, S.FORM_REF, o1, 3, flush, stream)
         plain = g.n / (float(pp.mean()) * 1e-3)
+        # the plain form end to end: one field from pinned host memory through
+        # sal_solve_host (copy in, solve, copy both components out, wait)
+        h1 = torch.tensor(h[:1]).pin_memory()
+        r1 = (torch.empty_like(h1).pin_memory(), torch.empty_like(h1).pin_memory())
+        grid.solve_host(h1.numpy(), r1[0].numpy(), r1[1].numpy(), S.FORM_REF)
+        t1 = time.perf_counter()
+        for _ in range(3):
+            grid.solve_host(h1.numpy(), r1[0].numpy(), r1[1].numpy(), S.FORM_REF)
+        plain_e2e = g.n * 3 / (time.perf_counter() - t1)
 
     # ---- end to end through the host-buffer C ABI (pinned buffers).  Each step
     # copies its fields in, solves and copies both components out.  The
@@ -412,8 +548,10 @@ def main():
             "latency_ms": {"p50": float(np.percentile(per, 50)), "p99": float(np.percentile(per, 99))},
             "accuracy": {"rel_l2_vs_fp64_direct_max": max(rels), "rel_l2_vs_fp64_direct_mean": float(np.mean(rels)),
                          "max_err_over_max_ref": max(mxs), "fields_checked": len(rels), "targets": len(tg)},
-            "plain_fp64": None if plain is None else {"value": plain, "unit": "evals/s",
-                                                      "batched_over_plain": value / world / plain},
+            "plain_fp64": None if plain is None else {
+                "value": plain, "unit": "evals/s", "batched_over_plain": value / world / plain,
+                "e2e": {"value": plain_e2e, "unit": "evals/s", "api": "sal_solve_host, SAL_FORM_REF, one field",
+                        "h2d_bytes_per_step": 8 * g.n, "d2h_bytes_per_step": 16 * g.n}},
             "roofline": roof,
             "work": {k: st[k] for k in ("pairs_pp", "pairs_pc", "pairs_cp", "pairs_cc", "macs_up", "macs_down")},
             "setup_s": {"grid_generation": t_gen, "tree_and_lists": t_lists, "plan_and_upload": st["setup_seconds"]},

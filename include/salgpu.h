@@ -134,6 +134,16 @@ int sal_grid_stats_get(const sal_grid *g, sal_grid_stats *s);
  * check. */
 int sal_grid_sync(sal_grid *g, void *stream);
 
+/* Fault injection for tests of the device-side time-outs (no counterpart in
+ * the reference).  polls > 0: in the next FP64 solve on the grid, the leaf
+ * pass leaves the last staging copy of every target group unissued and bounds
+ * each staging wait to `polls` polls, so every group's last wait runs out
+ * with no copy in flight.  That solve's outputs are undefined, and the next
+ * sal_grid_sync (or the host entry point that ran the solve) returns
+ * SAL_ETIMEOUT and clears the flag; later solves are unaffected.  polls = 0
+ * cancels a pending injection. */
+int sal_grid_inject_timeout(sal_grid *g, int32_t polls);
+
 /* Per-pass device timers.  enable = 1 turns them on (each FP64 solve then
  * records CUDA events on its stream around three passes and waits for the
  * last), 0 turns them off, -1 leaves them as they are; 1 and 0 also reset the
@@ -143,13 +153,16 @@ int sal_grid_sync(sal_grid *g, void *stream);
 int sal_grid_timing(sal_grid *g, int32_t enable, double *phase_ms, int64_t *solves);
 
 /* CUDA graphs of batched solves (no counterpart in the reference, which
- * solves one field per run).  enable = 1: the first SAL_FORM_MIXED
- * sal_solve of each call shape (field and output pointers, nfields, leading
- * dimensions) on a non-NULL stream runs as usual and is then captured into a
- * graph, on a stream of the caller stream's priority; later solves of that
- * shape launch the graph on their stream.  The grid keeps up to 128 graphs,
- * dropping the oldest.  0 frees them and solves launch kernel by kernel again.
- * Graphs are not used while the per-pass timers are on. */
+ * solves one field per run).  enable = 1: the second SAL_FORM_MIXED sal_solve
+ * of a call shape (field and output pointers, nfields, leading dimensions) on
+ * a non-NULL stream runs as usual and is then captured into a graph, on a
+ * stream of the caller stream's priority; later solves of that shape launch
+ * the graph on their stream.  Graphs therefore pay off only for callers that
+ * reuse their buffers.  The grid keeps up to 128 graphs, dropping the oldest.
+ * 0 frees them and solves launch kernel by kernel again.  Graphs are not used
+ * while the per-pass timers are on.  The graph cache has a lock of its own;
+ * other state of a grid (its batched buffers) is shared by its solves, so one
+ * grid's solves must not run concurrently on different streams. */
 int sal_grid_set_graphs(sal_grid *g, int32_t enable);
 
 /* Throughput of the FP64 (precision 64) or FP32 (precision 32) fused
@@ -226,7 +239,9 @@ int sal_direct_sum(const double *xs, const double *ys, const double *zs, const d
  * library's device memory that every GPU loading the library keeps until the
  * process exits.  nt above SAL_NOALLOC_SCRATCH_DOUBLES / 2 returns SAL_EINVAL.
  * The first call on a device looks up that array's device address (make it
- * before any stream capture).  All calls share the array: calls whose work
+ * before any stream capture) and keeps it for the rest of the process: after
+ * a cudaDeviceReset of that device the kept address is stale, so do not reset
+ * a device between calls.  All calls share the array: calls whose work
  * overlaps on the GPU race and must be ordered by the caller (one stream, or
  * events). */
 int sal_direct_sum_noalloc(const double *xs, const double *ys, const double *zs, const double *w, int32_t n,

@@ -68,9 +68,9 @@ def lib():
     L.or_free.argtypes = [vp]
     L.or_fast_sum.argtypes = [_dp, _dp, _ip, i, vp, _dp, _dp, _dp, _dp, _dp, i, i, i]
     L.or_fast_sum_cart.argtypes = [_dp, _dp, _ip, i, vp, _dp, _dp, _dp, _dp, _dp, i, i, i]
-    L.or_proxy_source_compute.argtypes = [_dp, vp, _ip, i, _dp, _dp, _dp, _dp, _dp, i, i, i]
-    L.or_pc_compute.argtypes = [_dp, _dp, _ip, i, vp, _dp, _dp, _dp, i, _dp]
-    L.or_pp_compute.argtypes = [_dp, _dp, _ip, i, vp, _dp, _dp, _dp, _dp, _dp]
+    L.or_proxy_source_compute.argtypes = [_dp, vp, _ip, i, _dp, _dp, _dp, _dp, _dp, i, i, i, i]
+    L.or_pc_compute.argtypes = [_dp, _dp, _ip, i, vp, _dp, _dp, _dp, i, _dp, i, i]
+    L.or_pp_compute.argtypes = [_dp, _dp, _ip, i, vp, _dp, _dp, _dp, _dp, _dp, i, i]
     L.or_direct_sum.argtypes = [_dp, _dp, _dp, _dp, _dp, i, _ip, i, _dp, _dp, i]
     L.or_dtt_work.argtypes = [vp, _ip, i, i, _dp, C.POINTER(d)]
     _lib = L
@@ -226,43 +226,48 @@ def fast_sum_cart(tree: Tree, inter: np.ndarray, xs, ys, zs, area, ssh, degree, 
     return ox, oy
 
 
-def proxy_source_compute(tree: Tree, points_panels, xs, ys, zs, sshs, areas, degree, transposed=True):
-    """mom6_fast_sum_module.f90:33-74; transposed=True is the reference's store."""
+def proxy_source_compute(tree: Tree, points_panels, xs, ys, zs, sshs, areas, degree, transposed=True,
+                         nthreads=1):
+    """mom6_fast_sum_module.f90:33-74; transposed=True is the reference's store.
+    Threads own disjoint panel ranges; every weight sums its points in the
+    reference's order for any thread count."""
     nlev = points_panels.shape[0]
     P = (degree + 1) ** 2
     w = np.zeros(P * tree.npanels)
     ppf = _i32(np.asfortranarray(points_panels).reshape(-1, order="F"))
     lib().or_proxy_source_compute(w, tree.handle, ppf, nlev, _f64(xs), _f64(ys), _f64(zs), _f64(sshs),
-                                  _f64(areas), int(degree), len(xs), int(bool(transposed)))
+                                  _f64(areas), int(degree), len(xs), int(bool(transposed)), int(nthreads))
     return w
 
 
-def pc_compute(tree: Tree, pc, xs, ys, zs, degree, weights, out=None):
-    """mom6_fast_sum_module.f90:153-174."""
+def pc_compute(tree: Tree, pc, xs, ys, zs, degree, weights, out=None, nthreads=1):
+    """mom6_fast_sum_module.f90:153-174.  Threads own disjoint target ranges
+    (as the reference's ranks own points); each target sums its entries in list
+    order for any thread count."""
     n = len(xs)
     ox, oy = (np.zeros(n), np.zeros(n)) if out is None else out
     lib().or_pc_compute(ox, oy, _i32(pc.reshape(-1)), len(pc), tree.handle, _f64(xs), _f64(ys), _f64(zs),
-                        int(degree), _f64(weights))
+                        int(degree), _f64(weights), n, int(nthreads))
     return ox, oy
 
 
-def pp_compute(tree: Tree, pp, xs, ys, zs, areas, sshs, out=None):
-    """mom6_fast_sum_module.f90:177-192 at one rank."""
+def pp_compute(tree: Tree, pp, xs, ys, zs, areas, sshs, out=None, nthreads=1):
+    """mom6_fast_sum_module.f90:177-192 at one rank (threads as in pc_compute)."""
     n = len(xs)
     ox, oy = (np.zeros(n), np.zeros(n)) if out is None else out
     lib().or_pp_compute(ox, oy, _i32(pp.reshape(-1)), len(pp), tree.handle, _f64(xs), _f64(ys), _f64(zs),
-                        _f64(areas), _f64(sshs))
+                        _f64(areas), _f64(sshs), n, int(nthreads))
     return ox, oy
 
 
-def mom6_solve(xs, ys, zs, areas, sshs, theta, thresh, degree, transposed=True):
+def mom6_solve(xs, ys, zs, areas, sshs, theta, thresh, degree, transposed=True, nthreads=1):
     """The mom6_code.f90 solve sequence at one rank (:177-312)."""
     tree = tree_traverse(xs, ys, zs, thresh)
     ppan = assign_points_to_panels(tree, xs, ys, zs)
     pc, pp = single_tree_traversal(tree, theta, thresh, xs, ys, zs)
-    w = proxy_source_compute(tree, ppan, xs, ys, zs, sshs, areas, degree, transposed)
-    ox, oy = pc_compute(tree, pc, xs, ys, zs, degree, w)
-    pp_compute(tree, pp, xs, ys, zs, areas, sshs, out=(ox, oy))
+    w = proxy_source_compute(tree, ppan, xs, ys, zs, sshs, areas, degree, transposed, nthreads)
+    ox, oy = pc_compute(tree, pc, xs, ys, zs, degree, w, nthreads=nthreads)
+    pp_compute(tree, pp, xs, ys, zs, areas, sshs, out=(ox, oy), nthreads=nthreads)
     return ox, oy
 
 

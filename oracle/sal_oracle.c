@@ -755,15 +755,24 @@ void or_fast_sum_cart(double *slon, double *slat, const int *list, int ninter, c
  * orientation pc_interact expects.  Adds into weights (P*npanels). */
 void or_proxy_source_compute(double *weights, const or_tree *t, const int *points_panels, int nlev,
                              const double *xs, const double *ys, const double *zs, const double *sshs,
-                             const double *areas, int d, int point_count, int transposed)
+                             const double *areas, int d, int point_count, int transposed, int nthreads)
 {
     int n = d + 1;
+    if (nthreads < 1) nthreads = 1;
+    /* Threads own disjoint panel-id ranges (the panels' weights they write);
+     * each walks every point in order, so every weight sums its points in the
+     * reference's order whatever the thread count. */
+#pragma omp parallel num_threads(nthreads)
+    {
+    int nth = omp_get_num_threads(), me = omp_get_thread_num();
+    int lo = (int)((long long)t->np * me / nth) + 1, hi = (int)((long long)t->np * (me + 1) / nth);
     double bv[64 * 64];
     for (int i = 1; i <= point_count; ++i) {
         double x = xs[i - 1], y = ys[i - 1], z = zs[i - 1], a = areas[i - 1], h = sshs[i - 1];
         for (int j = 1; j <= nlev; ++j) {
             int it = points_panels[(size_t)(j - 1) + (size_t)nlev * (size_t)(i - 1)];
             if (it == -1) break;
+            if (it < lo || it > hi) continue;
             const or_panel *P = &t->p[it - 1];
             size_t shift = (size_t)(it - 1) * (size_t)(n * n);
             double xi, eta;
@@ -778,16 +787,26 @@ void or_proxy_source_compute(double *weights, const or_tree *t, const int *point
                 }
         }
     }
+    }
 }
 
 /* pc_compute + pc_interact, mom6_fast_sum_module.f90:153-174, :76-107.
  * pc holds npc pairs (target point id, source panel id). */
 void or_pc_compute(double *slon, double *slat, const int *pc, int npc, const or_tree *t, const double *xs,
-                   const double *ys, const double *zs, int d, const double *weights)
+                   const double *ys, const double *zs, int d, const double *weights, int npoints, int nthreads)
 {
     int n = d + 1;
+    if (nthreads < 1) nthreads = 1;
+    /* Threads own disjoint target-point ranges, as MPI ranks own points in
+     * mom6_code.f90; each walks the whole list in order, so every target sums
+     * its entries in list order whatever the thread count. */
+#pragma omp parallel num_threads(nthreads)
+    {
+    int nth = omp_get_num_threads(), me = omp_get_thread_num();
+    int lo = (int)((long long)npoints * me / nth) + 1, hi = (int)((long long)npoints * (me + 1) / nth);
     for (int e = 0; e < npc; ++e) {
         int it = pc[2 * e], is = pc[2 * e + 1];
+        if (it < lo || it > hi) continue;
         const or_panel *S = &t->p[is - 1];
         const double *W = weights + (size_t)(is - 1) * (size_t)(n * n);
         double cxn[64], cen[64];
@@ -807,15 +826,24 @@ void or_pc_compute(double *slon, double *slat, const int *pc, int npc, const or_
             }
         }
     }
+    }
 }
 
 /* pp_compute + pp_interact, mom6_fast_sum_module.f90:177-192, :109-150, at one
  * rank (relabeled_points_inside == points_inside, no halo points). */
 void or_pp_compute(double *slon, double *slat, const int *pp, int npp, const or_tree *t, const double *xs,
-                   const double *ys, const double *zs, const double *areas, const double *sshs)
+                   const double *ys, const double *zs, const double *areas, const double *sshs, int npoints,
+                   int nthreads)
 {
+    if (nthreads < 1) nthreads = 1;
+    /* target-point ownership per thread, as in or_pc_compute */
+#pragma omp parallel num_threads(nthreads)
+    {
+    int nth = omp_get_num_threads(), me = omp_get_thread_num();
+    int lo = (int)((long long)npoints * me / nth) + 1, hi = (int)((long long)npoints * (me + 1) / nth);
     for (int e = 0; e < npp; ++e) {
         int it = pp[2 * e], is = pp[2 * e + 1];
+        if (it < lo || it > hi) continue;
         const or_panel *S = &t->p[is - 1];
         double tx = xs[it - 1], ty = ys[it - 1], tz = zs[it - 1];
         for (int i = 0; i < S->count; ++i) {
@@ -825,6 +853,7 @@ void or_pp_compute(double *slon, double *slat, const int *pp, int npp, const or_
             slon[it - 1] = slon[it - 1] + sshs[s] * areas[s] * sx;
             slat[it - 1] = slat[it - 1] + sshs[s] * areas[s] * sy;
         }
+    }
     }
 }
 

@@ -109,7 +109,10 @@ struct GridImpl {
     };
     bool use_graphs = false;
     std::vector<GraphEntry> graphs;
+    std::vector<GraphShape> seen;     // shapes solved once: captured on their second solve
+    std::mutex graph_mu;              // guards use_graphs, graphs and seen
     double *h_w = nullptr;                                        // device, P*npanels
+    uint32_t inject_polls = 0;        // sal_grid_inject_timeout: applies to the next FP64 solve
     std::vector<void *> allocs;
     std::mutex mu;
     // optional per-pass timers: events recorded on the launching stream
@@ -146,6 +149,21 @@ static int dalloc(GridImpl &g, T **p, size_t count) {
     g.allocs.push_back(*p);
     g.bytes += (int64_t)(count * sizeof(T));
     return SAL_OK;
+}
+
+// Frees a buffer dalloc made for this grid and stops counting it.  The caller
+// has made sure no device work still reads or writes it.
+template <class T>
+static void dfree(GridImpl &g, T **p, size_t count) {
+    if (!*p) return;
+    for (size_t i = 0; i < g.allocs.size(); ++i)
+        if (g.allocs[i] == (void *)*p) {
+            g.allocs.erase(g.allocs.begin() + (std::ptrdiff_t)i);
+            g.bytes -= (int64_t)(count * sizeof(T));
+            break;
+        }
+    cudaFree(*p);
+    *p = nullptr;
 }
 
 template <class T>
@@ -372,6 +390,11 @@ static void solve_fp64(GridImpl &g, const double *ssh, double *ox, double *oy, i
     a.out_x = ox;
     a.out_y = oy;
     a.err = g.err;
+    if (g.inject_polls) {
+        a.polls = g.inject_polls;
+        a.skip_last = 1;
+        g.inject_polls = 0;
+    }
     dev::launch_eval(0, form, a, (int)pl.leaf_groups.size(), st);
     if (g.timing) {
         cudaEventRecord(g.ev[3], st);
@@ -593,12 +616,13 @@ static void solve_mixed_block(GridImpl &g, const double *ssh, int64_t ld_ssh, in
     }
 }
 
+constexpr size_t kMaxGraphs = 128;
+
 // Captures the batched solve of one call shape into a graph (nothing runs).
 // The capture stream takes the caller stream's priority, which the graph's
 // kernels keep.  Every allocation and kernel attribute the solve needs exists
-// already: the same shape has just run.
+// already: the same shape has just run.  Called with graph_mu held.
 static int capture_mixed(GridImpl &g, const GridImpl::GraphShape &k, cudaStream_t caller) {
-    constexpr size_t kMaxGraphs = 128;
     int prio = 0;
     CK(cudaStreamGetPriority(caller, &prio));
     cudaStream_t cs = nullptr;
@@ -625,11 +649,12 @@ static int capture_mixed(GridImpl &g, const GridImpl::GraphShape &k, cudaStream_
 extern "C" int sal_grid_set_graphs(sal_grid *G, int32_t enable) {
     if (!G) return set_error(SAL_EINVAL, "null argument");
     GridImpl &g = G->g;
-    std::lock_guard<std::mutex> lk(g.mu);
+    std::lock_guard<std::mutex> lk(g.graph_mu);
     CK(cudaSetDevice(g.dev));
     if (!enable) {
         for (auto &e : g.graphs) cudaGraphExecDestroy(e.exec);
         g.graphs.clear();
+        g.seen.clear();
     }
     g.use_graphs = enable != 0;
     return SAL_OK;
@@ -650,17 +675,35 @@ extern "C" int sal_solve(sal_grid *G, const double *ssh, int32_t nf, int64_t ld_
         const int FT = g.FT ? g.FT : (g.max_fields <= 32 ? 32 : 64);
         int rc = ensure_mixed(g, FT);
         if (rc) return rc;
-        const bool graph = g.use_graphs && st != nullptr && !g.timing;
         const GridImpl::GraphShape shape{ssh, nf, ld_ssh, ox, oy, ld_out};
-        if (graph)
-            for (const auto &e : g.graphs)
-                if (e.shape == shape) {
-                    CK(cudaGraphLaunch(e.exec, st));
-                    return SAL_OK;
-                }
+        bool graph = false;
+        {
+            // the lock keeps sal_grid_set_graphs from destroying a graph
+            // between its lookup and its launch
+            std::lock_guard<std::mutex> lk(g.graph_mu);
+            graph = g.use_graphs && st != nullptr && !g.timing;
+            if (graph)
+                for (const auto &e : g.graphs)
+                    if (e.shape == shape) {
+                        CK(cudaGraphLaunch(e.exec, st));
+                        return SAL_OK;
+                    }
+        }
         for (int f0 = 0; f0 < nf; f0 += FT) solve_mixed_block(g, ssh, ld_ssh, f0, nf, ox, oy, ld_out, st);
         CK(cudaGetLastError());
-        return graph ? capture_mixed(g, shape, st) : SAL_OK;
+        if (!graph) return SAL_OK;
+        // a shape is captured on its second solve, so callers that pass fresh
+        // buffers every call do not pay a capture per call
+        std::lock_guard<std::mutex> lk(g.graph_mu);
+        if (!g.use_graphs) return SAL_OK;
+        for (size_t i = 0; i < g.seen.size(); ++i)
+            if (g.seen[i] == shape) {
+                g.seen.erase(g.seen.begin() + (std::ptrdiff_t)i);
+                return capture_mixed(g, shape, st);
+            }
+        if (g.seen.size() >= kMaxGraphs) g.seen.erase(g.seen.begin());
+        g.seen.push_back(shape);
+        return SAL_OK;
     }
     for (int f = 0; f < nf; ++f)
         solve_fp64(g, ssh + (size_t)f * ld_ssh, ox + (size_t)f * ld_out, oy + (size_t)f * ld_out,
@@ -698,6 +741,13 @@ extern "C" int sal_grid_timing(sal_grid *G, int32_t enable, double *phase_ms, in
         for (double &v : g.phase_ms) v = 0;
         g.phase_solves = 0;
     }
+    return SAL_OK;
+}
+
+extern "C" int sal_grid_inject_timeout(sal_grid *G, int32_t polls) {
+    if (!G) return set_error(SAL_EINVAL, "null argument");
+    if (polls < 0) return set_error(SAL_EINVAL, "polls must be >= 0");
+    G->g.inject_polls = (uint32_t)polls;
     return SAL_OK;
 }
 
@@ -742,6 +792,14 @@ extern "C" int sal_solve_host(sal_grid *G, const double *ssh, int32_t nf, int64_
     std::lock_guard<std::mutex> lk(g.mu);
     CK(cudaSetDevice(g.dev));
     if (g.hb_fields < nf) {
+        // the old staging is too small: release it (after the grid's stream
+        // has finished with it) before taking a larger one
+        CK(cudaStreamSynchronize(g.stream));
+        const size_t old = (size_t)n * g.hb_fields;
+        dfree(g, &g.hb_ssh, old);
+        dfree(g, &g.hb_ox, old);
+        dfree(g, &g.hb_oy, old);
+        g.hb_fields = 0;
         int rc = dalloc(g, &g.hb_ssh, (size_t)n * nf);
         if (!rc) rc = dalloc(g, &g.hb_ox, (size_t)n * nf);
         if (!rc) rc = dalloc(g, &g.hb_oy, (size_t)n * nf);
@@ -782,7 +840,14 @@ extern "C" int sal_solve_host_async(sal_grid *G, const double *ssh, int32_t nf, 
     GridImpl::HostSlot &h = g.hslot[g.hnext];
     g.hnext ^= 1;
     if (h.fields < nf) {
+        // the slot's last copy out has read its results, which follow its
+        // solve: after that nothing uses the old buffers
         if (h.used) CK(cudaEventSynchronize(h.out));
+        const size_t old = (size_t)n * (size_t)h.fields;
+        dfree(g, &h.ssh, old);
+        dfree(g, &h.ox, old);
+        dfree(g, &h.oy, old);
+        h.fields = 0;
         int rc = dalloc(g, &h.ssh, (size_t)n * nf);
         if (!rc) rc = dalloc(g, &h.ox, (size_t)n * nf);
         if (!rc) rc = dalloc(g, &h.oy, (size_t)n * nf);

@@ -52,10 +52,12 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
         : "memory");
     return ok != 0;
 }
-// Bounded wait: gives up after a fixed number of polls and raises the grid's
-// error flag, so a copy that never lands cannot hang the GPU.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity, int *err) {
-    for (uint32_t it = 0; it < (1u << 24); ++it)
+// Bounded wait: gives up after `polls` polls and raises the grid's error
+// flag, so a copy that never lands cannot hang the GPU.
+constexpr uint32_t kDefaultPolls = 1u << 24;
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity, int *err,
+                                                  uint32_t polls = kDefaultPolls) {
+    for (uint32_t it = 0; it < polls; ++it)
         if (mbar_try_wait(bar, parity)) return true;
     atomicExch(err, kErrTimeout);
     return false;
@@ -203,6 +205,8 @@ struct EvalArgs {
     double *out_x, *out_y;   // leaf groups: caller order, overwritten
     double4 *partial;        // proxy groups: P outputs per unit
     int *err;
+    uint32_t polls;          // poll limit of every staging wait (0: kDefaultPolls)
+    int skip_last;           // fault injection: the last item's copy of every group is not issued
 };
 
 struct UpArgs {

@@ -33,7 +33,10 @@ double *g_scratch_ptr[kMaxDevices] = {nullptr};
 
 // Device address of the scratch array on the current device.  In host code
 // g_noalloc_scratch names a host-side stand-in, so the address is looked up
-// once per device (with that device current) and cached.
+// once per device (with that device current) and cached for the rest of the
+// process.  A cudaDeviceReset would recreate the device's context and leave
+// the cached address stale; the header tells callers not to reset a device
+// between calls.
 static int scratch_address(int dev, double **out) {
     std::lock_guard<std::mutex> lk(g_mu);
     if (!g_scratch_ptr[dev]) {

@@ -37,7 +37,7 @@ EXPORTS = (
     "sal_grid_create", "sal_grid_stats_get", "sal_grid_sync", "sal_grid_destroy", "sal_solve", "sal_fast_sum_host",
     "sal_proxy_source_compute_host", "sal_pc_compute_host", "sal_pp_compute_host", "sal_direct_sum",
     "sal_grid_timing", "sal_fma_peak", "sal_direct_sum_noalloc", "sal_solve_host", "sal_solve_host_async",
-    "sal_solve_host_wait", "sal_grid_set_graphs",
+    "sal_solve_host_wait", "sal_grid_set_graphs", "sal_grid_inject_timeout",
 )
 
 
@@ -108,6 +108,7 @@ def lib():
         L.sal_solve_host_async.argtypes = [vp, vp, i32, i64, vp, vp, i64, i32]
         L.sal_solve_host_wait.argtypes = [vp]
         L.sal_grid_set_graphs.argtypes = [vp, i32]
+        L.sal_grid_inject_timeout.argtypes = [vp, i32]
         L.sal_proxy_source_compute_host.argtypes = [vp, vp, vp]
         L.sal_pc_compute_host.argtypes = [vp, vp, vp, vp]
         L.sal_pp_compute_host.argtypes = [vp, vp, vp, vp]
@@ -317,6 +318,12 @@ class Grid:
         outputs overwritten.  Pinned arrays make the copies asynchronous."""
         F = ssh.shape[0] if ssh.ndim == 2 else 1
         _check(lib().sal_solve_host(self.handle, _ptr(ssh), F, self.n, _ptr(out_x), _ptr(out_y), self.n, int(form)))
+
+    def inject_timeout(self, polls):
+        """Test hook (sal_grid_inject_timeout): the next FP64 solve's leaf
+        pass gives up a staging wait on every group after `polls` polls; the
+        host then sees SAL_ETIMEOUT."""
+        _check(lib().sal_grid_inject_timeout(self.handle, int(polls)))
 
     def set_graphs(self, enable=True):
         """CUDA graphs of batched solves, one per call shape (sal_grid_set_graphs):

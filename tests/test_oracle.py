@@ -214,3 +214,21 @@ def test_cartesian_dtt_converges_spectrally(small):
     assert e[0] > e[1] > e[2] and e[2] < 1e-6
     e_ref = rel_l2(*O.fast_sum(t, L, g.xs, g.ys, g.zs, g.areas, h, 8, 4), dx, dy)
     assert e_ref > 10 * e[2]
+
+
+def test_mom6_thread_split_is_bitwise_serial(small):
+    """Threads that own disjoint panels (weights) or targets (pc/pp sums) keep
+    every sum in the reference's order, so any thread count gives the serial
+    result bit for bit."""
+    g, h, t = small
+    ppan = O.assign_points_to_panels(t, g.xs, g.ys, g.zs)
+    pc, pp = O.single_tree_traversal(t, 0.7, 20, g.xs, g.ys, g.zs)
+    w1 = O.proxy_source_compute(t, ppan, g.xs, g.ys, g.zs, h, g.areas, 8, True, nthreads=1)
+    w5 = O.proxy_source_compute(t, ppan, g.xs, g.ys, g.zs, h, g.areas, 8, True, nthreads=5)
+    assert np.array_equal(w1, w5)
+    a = O.pc_compute(t, pc, g.xs, g.ys, g.zs, 8, w1, nthreads=1)
+    b = O.pc_compute(t, pc, g.xs, g.ys, g.zs, 8, w1, nthreads=5)
+    assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+    a = O.pp_compute(t, pp, g.xs, g.ys, g.zs, g.areas, h, nthreads=1)
+    b = O.pp_compute(t, pp, g.xs, g.ys, g.zs, g.areas, h, nthreads=5)
+    assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
