@@ -34,6 +34,7 @@ extern "C" {
 #define SAL_ECUDA (-3)
 #define SAL_ETIMEOUT (-4)
 #define SAL_ENODEV (-5)
+#define SAL_ETREE (-6)   /* panels given without points_inside differ from the tree of the coordinates */
 
 /* Evaluator families.  DTT is the code.f90 path (fast_sum_module.f90); the two
  * STT modes are the mom6_code.f90 path (mom6_fast_sum_module.f90). */
@@ -218,6 +219,69 @@ int sal_pc_compute_host(sal_grid *g, const double *proxy_weights, double *sal_x,
 
 /* pp_compute, mom6_fast_sum_module.f90:177-192 (one rank, no halo points). */
 int sal_pp_compute_host(sal_grid *g, const double *sshs, double *sal_x, double *sal_y);
+
+/* ------------------------------------------------------------------ reference-signature entry points
+ * The four hot routines with the reference's argument lists, for a Fortran
+ * ISO_C_BINDING front end that changes nothing in code.f90 / mom6_code.f90
+ * but their `use` lines.  Fortran derived types are not interoperable, so the
+ * cube_panel array arrives flattened as in sal_tree_import (npanels, ints9,
+ * dbl7, pt_off); pt_idx (points_inside) may be NULL, in which case the tree is
+ * rebuilt from the coordinates and must equal the given panels (else
+ * SAL_ETREE: pass pt_idx).  interaction_pair lists arrive as int32 tuples.
+ * Each call hashes its set-up arguments (coordinates, areas, panels, list,
+ * degree) and reuses the device grid it built for the same contents; any
+ * change builds a new grid.  The library keeps up to four grids per entry
+ * point, least recently used dropped.  Outputs are added into the caller's
+ * arrays (intent(inout)), on the current CUDA device, synchronously.  The
+ * calls serialise on one process-wide lock. */
+
+/* fast_sum, fast_sum_module.f90:291-332 (list: list_count triplets target
+ * panel, source panel, type).  Only interactions i (1-based) with
+ * MOD(i, process_count) == rank are evaluated, as in the reference
+ * (:303-304), so the caller's Sum_Array still completes the sum.  Arithmetic
+ * form: sal_dropin_config (SAL_FORM_REF unless changed). */
+int sal_fast_sum(double *sal_longrad, double *sal_latgrad, const int32_t *interaction_list, int64_t list_count,
+                 int32_t npanels, const int32_t *ints9, const double *dbl7, const int64_t *pt_off,
+                 const int32_t *pt_idx, const double *xs, const double *ys, const double *zs, const double *area,
+                 const double *ssh, int32_t point_count, int32_t interp_degree, int32_t rank, int32_t process_count);
+
+/* proxy_source_compute, mom6_fast_sum_module.f90:33-74: adds the proxy
+ * source weights ((d+1)^2 * npanels, panel-major) into
+ * proxy_source_weights.  points_panels is (nlev x point_count) column-major,
+ * as assign_points_to_panels fills it (tree_module.f90:249-273); it must
+ * match the panels.  Weight orientation: sal_dropin_config (the reference's
+ * transposed store unless changed). */
+int sal_mom6_proxy_source_compute(double *proxy_source_weights, int32_t npanels, const int32_t *ints9,
+                                  const double *dbl7, const int64_t *pt_off, const int32_t *pt_idx,
+                                  const int32_t *points_panels, int32_t nlev, const double *xs, const double *ys,
+                                  const double *zs, const double *sshs, const double *areas, int32_t interp_degree,
+                                  int32_t point_count);
+
+/* pc_compute, mom6_fast_sum_module.f90:153-174 (list: pc_count pairs target
+ * point, source panel; point_count = size(xs)). */
+int sal_mom6_pc_compute(double *sal_longrad, double *sal_latgrad, const int32_t *pc_interaction_list, int64_t pc_count,
+                        int32_t npanels, const int32_t *ints9, const double *dbl7, const int64_t *pt_off,
+                        const int32_t *pt_idx, const double *xs, const double *ys, const double *zs,
+                        int32_t point_count, int32_t interp_degree, const double *proxy_weights);
+
+/* pp_compute, mom6_fast_sum_module.f90:177-192 (list: pp_count pairs target
+ * point, source panel).  One rank: the halo arrays e_* of other ranks' points
+ * must be empty (extra_count 0), else SAL_EINVAL. */
+int sal_mom6_pp_compute(double *sal_longrad, double *sal_latgrad, const int32_t *pp_interaction_list, int64_t pp_count,
+                        int32_t npanels, const int32_t *ints9, const double *dbl7, const int64_t *pt_off,
+                        const int32_t *pt_idx, const double *xs, const double *ys, const double *zs,
+                        const double *areas, const double *sshs, const double *e_xs, const double *e_ys,
+                        const double *e_zs, const double *e_areas, const double *e_sshs, int32_t extra_count,
+                        int32_t own_points);
+
+/* Settings of the four entry points above (no counterpart in the reference):
+ * form is SAL_FORM_REF (default) or SAL_FORM_ACCURATE for sal_fast_sum;
+ * mom6_mode is SAL_MODE_STT_REF_COMPAT (default, the reference's transposed
+ * weights) or SAL_MODE_STT_CORRECT for sal_mom6_proxy_source_compute. */
+int sal_dropin_config(int32_t form, int32_t mom6_mode);
+
+/* Frees every grid the four entry points above keep. */
+int sal_dropin_release(void);
 
 /* FP64 direct O(N^2) sum at nt targets (0-based indices into the sources),
  * with the reference kernel in its own operation order.  Device pointers;

@@ -26,7 +26,7 @@ import numpy as np
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libsalgpu.so")
 
-SAL_OK, SAL_EINVAL, SAL_ENOMEM, SAL_ECUDA, SAL_ETIMEOUT, SAL_ENODEV = 0, -1, -2, -3, -4, -5
+SAL_OK, SAL_EINVAL, SAL_ENOMEM, SAL_ECUDA, SAL_ETIMEOUT, SAL_ENODEV, SAL_ETREE = 0, -1, -2, -3, -4, -5, -6
 MODE_DTT, MODE_STT_REF_COMPAT, MODE_STT_CORRECT = 0, 1, 2
 FORM_REF, FORM_ACCURATE, FORM_MIXED = 0, 1, 2
 
@@ -37,7 +37,9 @@ EXPORTS = (
     "sal_grid_create", "sal_grid_stats_get", "sal_grid_sync", "sal_grid_destroy", "sal_solve", "sal_fast_sum_host",
     "sal_proxy_source_compute_host", "sal_pc_compute_host", "sal_pp_compute_host", "sal_direct_sum",
     "sal_grid_timing", "sal_fma_peak", "sal_direct_sum_noalloc", "sal_solve_host", "sal_solve_host_async",
-    "sal_solve_host_wait", "sal_grid_set_graphs", "sal_grid_inject_timeout",
+    "sal_solve_host_wait", "sal_grid_set_graphs", "sal_grid_inject_timeout", "sal_fast_sum",
+    "sal_mom6_proxy_source_compute", "sal_mom6_pc_compute", "sal_mom6_pp_compute", "sal_dropin_config",
+    "sal_dropin_release",
 )
 
 
@@ -116,6 +118,12 @@ def lib():
         L.sal_grid_timing.argtypes = [vp, i32, C.POINTER(d), C.POINTER(i64)]
         L.sal_fma_peak.argtypes = [i32, C.POINTER(d)]
         L.sal_direct_sum_noalloc.argtypes = [vp, vp, vp, vp, i32, vp, i32, vp, vp, vp]
+        L.sal_fast_sum.argtypes = [vp, vp, vp, i64, i32, vp, vp, vp, vp, vp, vp, vp, vp, vp, i32, i32, i32, i32]
+        L.sal_mom6_proxy_source_compute.argtypes = [vp, i32, vp, vp, vp, vp, vp, i32, vp, vp, vp, vp, vp, i32, i32]
+        L.sal_mom6_pc_compute.argtypes = [vp, vp, vp, i64, i32, vp, vp, vp, vp, vp, vp, vp, i32, i32, vp]
+        L.sal_mom6_pp_compute.argtypes = [vp, vp, vp, i64, i32, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp,
+                                          vp, vp, i32, i32]
+        L.sal_dropin_config.argtypes = [i32, i32]
         _lib = L
         return L
 
@@ -396,68 +404,97 @@ def direct_sum(xs, ys, zs, w, targets, stream=None):
 
 
 # ===================================================================== reference-named entry points
-# Grids are cached per (tree, list, degree, mode, rank split) so that repeated
-# calls with the same setup reuse the device-resident plan, as the Fortran
-# shim does (include/salgpu.h: sal_grid_create once per grid).
-_grid_cache: dict = {}
+# The reference's four hot routines with its argument lists, through the
+# library's reference-signature entry points (include/salgpu.h): each call
+# hands over the flattened cube_panel array, the list and the point arrays;
+# the library reuses the device grid it built for the same contents.
+
+def _flat_panels(cube_panels, with_points=True):
+    """(npanels, ints9, dbl7, pt_off, pt_idx or None) of a Tree or of a dict
+    in the Tree.export() layout (the cube_panel array of tree_module.f90:5-28)."""
+    e = cube_panels.export() if isinstance(cube_panels, Tree) else cube_panels
+    npn = len(e["level"])
+    ints = _i32(np.column_stack([e["level"], e["is_leaf"], e["id"], e["parent"], e["child"], e["face"]]).reshape(-1))
+    dbl = _f64(np.asarray(e["bounds"]).reshape(-1))
+    off = np.ascontiguousarray(e["pt_off"], dtype=np.int64)
+    idx = _i32(e["pt_idx"]) if with_points else None
+    return npn, ints, dbl, off, idx
 
 
-def _cache_key(*parts):
-    key = []
-    for p in parts:
-        if isinstance(p, np.ndarray):
-            key.append((p.shape, hash(p.tobytes())))
-        else:
-            key.append(id(p) if isinstance(p, Tree) else p)
-    return tuple(key)
+def _panel_ptrs(fp):
+    npn, ints, dbl, off, idx = fp
+    return [npn, _ptr(ints), _ptr(dbl), _ptr(off), None if idx is None else _ptr(idx)]
 
 
-def fast_sum(sal_longrad, sal_latgrad, interaction_list, cube_panels: Tree, xs, ys, zs, area, ssh, point_count,
-             interp_degree, rank=0, process_count=1, form=FORM_REF, device=0):
+def dropin_config(form=FORM_REF, mom6_mode=MODE_STT_REF_COMPAT):
+    """Arithmetic form of fast_sum (FORM_REF or FORM_ACCURATE) and proxy-weight
+    orientation of proxy_source_compute (MODE_STT_REF_COMPAT, the reference's
+    transposed store, or MODE_STT_CORRECT)."""
+    _check(lib().sal_dropin_config(int(form), int(mom6_mode)))
+
+
+def dropin_release():
+    """Frees the device grids the reference-named entry points keep."""
+    _check(lib().sal_dropin_release())
+
+
+def fast_sum(sal_longrad, sal_latgrad, interaction_list, cube_panels, xs, ys, zs, area, ssh, point_count,
+             interp_degree, rank=0, process_count=1, with_points_inside=True):
     """fast_sum_module.f90:291-332.  Adds into sal_longrad/sal_latgrad
-    (intent(inout)).  With process_count > 1 only interactions i with
-    MOD(i, process_count) == rank are evaluated (:303-304), so the MPI
+    (intent(inout), float64 arrays).  With process_count > 1 only interactions i
+    with MOD(i, process_count) == rank are evaluated (:303-304), so the MPI
     Sum_Array that follows in code.f90:99-100 still yields the full sum."""
-    L = np.asarray(interaction_list).reshape(-1, 3)
-    if process_count > 1:
-        i = np.arange(1, len(L) + 1)
-        L = L[(i % process_count) == rank]
-    L = _i32(L)
-    key = _cache_key(cube_panels, L, int(interp_degree), MODE_DTT, device, _f64(area)[:1].tobytes())
-    g = _grid_cache.get(key)
-    if g is None:
-        g = Grid(cube_panels, xs, ys, zs, area, interp_degree, MODE_DTT, L, device=device)
-        _grid_cache[key] = g
-    g.fast_sum_host(ssh, sal_longrad, sal_latgrad, form)
+    L = _i32(np.asarray(interaction_list).reshape(-1))
+    xs, ys, zs, area, ssh = _f64(xs), _f64(ys), _f64(zs), _f64(area), _f64(ssh)
+    fp = _flat_panels(cube_panels, with_points_inside)
+    _check(lib().sal_fast_sum(_ptr(sal_longrad), _ptr(sal_latgrad), _ptr(L), len(L) // 3, *_panel_ptrs(fp),
+                              _ptr(xs), _ptr(ys), _ptr(zs), _ptr(area), _ptr(ssh), int(point_count),
+                              int(interp_degree), int(rank), int(process_count)))
 
 
-def _stt_grid(tree, pc, pp, xs, ys, zs, areas, degree, mode, device):
-    pc, pp = _i32(np.asarray(pc).reshape(-1, 2)), _i32(np.asarray(pp).reshape(-1, 2))
-    key = _cache_key(tree, pc, pp, int(degree), int(mode), device)
-    g = _grid_cache.get(key)
-    if g is None:
-        g = Grid(tree, xs, ys, zs, areas, degree, mode, pc_list=pc, pp_list=pp, device=device)
-        _grid_cache[key] = g
-    return g
+def proxy_source_compute(proxy_source_weights, tree_panels, points_panels, xs, ys, zs, sshs, areas, interp_degree,
+                         point_count, with_points_inside=True):
+    """mom6_fast_sum_module.f90:33-74: adds the proxy source weights
+    ((d+1)^2 * npanels, panel-major) into proxy_source_weights.  points_panels
+    is (nlev, N) as assign_points_to_panels returns it."""
+    pp = np.asarray(points_panels)
+    nlev = pp.shape[0]
+    ppf = _i32(pp.reshape(-1, order="F"))
+    xs, ys, zs, sshs, areas = _f64(xs), _f64(ys), _f64(zs), _f64(sshs), _f64(areas)
+    fp = _flat_panels(tree_panels, with_points_inside)
+    _check(lib().sal_mom6_proxy_source_compute(_ptr(proxy_source_weights), *_panel_ptrs(fp), _ptr(ppf), nlev,
+                                               _ptr(xs), _ptr(ys), _ptr(zs), _ptr(sshs), _ptr(areas),
+                                               int(interp_degree), int(point_count)))
+
+
+def pc_compute(sal_longrad, sal_latgrad, pc_interaction_list, cube_panels, xs, ys, zs, interp_degree, proxy_weights,
+               with_points_inside=True):
+    """mom6_fast_sum_module.f90:153-174: adds the particle-cluster far field."""
+    L = _i32(np.asarray(pc_interaction_list).reshape(-1))
+    xs, ys, zs, w = _f64(xs), _f64(ys), _f64(zs), _f64(proxy_weights)
+    fp = _flat_panels(cube_panels, with_points_inside)
+    _check(lib().sal_mom6_pc_compute(_ptr(sal_longrad), _ptr(sal_latgrad), _ptr(L), len(L) // 2, *_panel_ptrs(fp),
+                                     _ptr(xs), _ptr(ys), _ptr(zs), len(xs), int(interp_degree), _ptr(w)))
+
+
+def pp_compute(sal_longrad, sal_latgrad, pp_interaction_list, cube_panels, xs, ys, zs, areas, sshs, e_xs=(), e_ys=(),
+               e_zs=(), e_areas=(), e_sshs=(), own_points=None, with_points_inside=True):
+    """mom6_fast_sum_module.f90:177-192: adds the near field.  One rank: the
+    halo arrays e_* of other ranks' points must be empty."""
+    L = _i32(np.asarray(pp_interaction_list).reshape(-1))
+    xs, ys, zs, areas, sshs = _f64(xs), _f64(ys), _f64(zs), _f64(areas), _f64(sshs)
+    ex = [_f64(a) for a in (e_xs, e_ys, e_zs, e_areas, e_sshs)]
+    own = len(xs) if own_points is None else int(own_points)
+    fp = _flat_panels(cube_panels, with_points_inside)
+    _check(lib().sal_mom6_pp_compute(_ptr(sal_longrad), _ptr(sal_latgrad), _ptr(L), len(L) // 2, *_panel_ptrs(fp),
+                                     _ptr(xs), _ptr(ys), _ptr(zs), _ptr(areas), _ptr(sshs),
+                                     *[_ptr(a) for a in ex], len(ex[0]), own))
 
 
 def mom6_grid(tree, pc_list, pp_list, xs, ys, zs, areas, interp_degree, ref_compat=True, device=0) -> Grid:
-    """The device grid behind proxy_source_compute / pc_compute / pp_compute."""
+    """A device grid of the mom6_code.f90 path with both lists, for the
+    Grid.proxy_source_compute_host / pc_compute_host / pp_compute_host
+    methods."""
     mode = MODE_STT_REF_COMPAT if ref_compat else MODE_STT_CORRECT
-    return _stt_grid(tree, pc_list, pp_list, xs, ys, zs, areas, interp_degree, mode, device)
-
-
-def proxy_source_compute(proxy_source_weights, grid: Grid, sshs):
-    """mom6_fast_sum_module.f90:33-74 on a grid from mom6_grid(): adds the
-    proxy source weights ((d+1)^2 * npanels, panel-major) into the array."""
-    grid.proxy_source_compute_host(sshs, proxy_source_weights)
-
-
-def pc_compute(sal_x, sal_y, grid: Grid, proxy_weights):
-    """mom6_fast_sum_module.f90:153-174: adds the particle-cluster far field."""
-    grid.pc_compute_host(proxy_weights, sal_x, sal_y)
-
-
-def pp_compute(sal_x, sal_y, grid: Grid, sshs):
-    """mom6_fast_sum_module.f90:177-192 at one rank: adds the near field."""
-    grid.pp_compute_host(sshs, sal_x, sal_y)
+    pc, pp = _i32(np.asarray(pc_list).reshape(-1, 2)), _i32(np.asarray(pp_list).reshape(-1, 2))
+    return Grid(tree, xs, ys, zs, areas, interp_degree, mode, pc_list=pc, pp_list=pp, device=device)

@@ -44,21 +44,21 @@ def test_mom6_lonlat_grid_matches_oracle_and_direct_sum():
     px, py = O.pp_compute(ot, pp, g.xs, g.ys, g.zs, g.areas, h)
     grid = S.mom6_grid(pt, pc, pp, g.xs, g.ys, g.zs, g.areas, d, ref_compat=True)
     w = np.zeros_like(w_ref)
-    S.proxy_source_compute(w, grid, h)
+    grid.proxy_source_compute_host(h, w)
     assert np.linalg.norm(w - w_ref) <= TOL_PARITY * np.linalg.norm(w_ref)
     gx, gy = np.zeros(g.n), np.zeros(g.n)
-    S.pc_compute(gx, gy, grid, w_ref)
+    grid.pc_compute_host(w_ref, gx, gy)
     assert rel_l2(gx, gy, ox, oy) <= TOL_PARITY
     qx, qy = np.zeros(g.n), np.zeros(g.n)
-    S.pp_compute(qx, qy, grid, h)
+    grid.pp_compute_host(h, qx, qy)
     assert rel_l2(qx, qy, px, py) <= TOL_PARITY
     # correct mode (untransposed weights) converges to the direct sum
     grid_c = S.mom6_grid(pt, pc, pp, g.xs, g.ys, g.zs, g.areas, d, ref_compat=False)
     wc = np.zeros_like(w_ref)
-    S.proxy_source_compute(wc, grid_c, h)
+    grid_c.proxy_source_compute_host(h, wc)
     cx, cy = np.zeros(g.n), np.zeros(g.n)
-    S.pc_compute(cx, cy, grid_c, wc)
-    S.pp_compute(cx, cy, grid_c, h)
+    grid_c.pc_compute_host(wc, cx, cy)
+    grid_c.pp_compute_host(h, cx, cy)
     tg = np.sort(np.random.default_rng(8).choice(g.n, 3000, replace=False)).astype(np.int32)
     T = lambda a: torch.tensor(a, device="cuda")
     dx, dy = S.direct_sum(T(g.xs), T(g.ys), T(g.zs), T(g.areas * h), T(tg))

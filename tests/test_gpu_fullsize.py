@@ -12,8 +12,9 @@ tests run the configurations' own grids:
 * cfg2, the whole list: the plain FP64 form, the accurate form and the batched
   form against the FP64 direct sum on 10,000 seeded targets.
 * cfg1, the 0.25 degree 1440 x 720 lon-lat grid (leaf 200, d = 8) in
-  ref_compat mode: proxy_source_compute over every panel, and pc_compute /
-  pp_compute at 4,000 seeded targets (the oracle evaluates every list entry of
+  ref_compat mode, through the reference-signature entry points:
+  proxy_source_compute over every panel, and pc_compute / pp_compute at 4,000
+  seeded targets (the oracle evaluates every list entry of
   those targets, so their sums are complete), against the oracle.  Bar:
   rel-L2 <= 1e-12.
 """
@@ -65,6 +66,7 @@ def test_cfg2_ref_form_matches_oracle_on_one_rank_share():
     pt = S.tree_traverse(g.xs, g.ys, g.zs, g.n, 200)
     gx, gy = np.zeros(g.n), np.zeros(g.n)
     S.fast_sum(gx, gy, L, pt, g.xs, g.ys, g.zs, g.areas, h, g.n, 8, rank=rank, process_count=P)
+    S.dropin_release()
     err = rel_l2(gx, gy, ox, oy)
     mx = float(np.max(np.hypot(gx - ox, gy - oy)) / np.max(np.hypot(ox, oy)))
     print(f"cfg2 REF form, share {rank} of {P} ({len(share)} interactions): rel-L2 {err:.3e}, max/max {mx:.3e}")
@@ -111,15 +113,19 @@ def test_cfg1_quarter_degree_mom6_ref_compat_matches_oracle():
     ppan = O.assign_points_to_panels(ot, g.xs, g.ys, g.zs)
     pc, pp = O.single_tree_traversal(ot, 0.7, thresh, g.xs, g.ys, g.zs)
     w_ref = O.proxy_source_compute(ot, ppan, g.xs, g.ys, g.zs, h, g.areas, d, transposed=True)
-    pt = S.tree_traverse(g.xs, g.ys, g.zs, g.n, thresh)
-    grid = S.mom6_grid(pt, pc, pp, g.xs, g.ys, g.zs, g.areas, d, ref_compat=True)
+    # the reference-signature entry points, with the oracle's own panels,
+    # points_panels and lists as a Fortran caller would pass them
+    panels = {k: getattr(ot, k) for k in ("level", "is_leaf", "id", "parent", "child", "face", "bounds",
+                                          "pt_off", "pt_idx")}
+    S.dropin_config(S.FORM_REF, S.MODE_STT_REF_COMPAT)
     w = np.zeros_like(w_ref)
-    S.proxy_source_compute(w, grid, h)
+    S.proxy_source_compute(w, panels, ppan, g.xs, g.ys, g.zs, h, g.areas, d, g.n)
     ew = float(np.linalg.norm(w - w_ref) / np.linalg.norm(w_ref))
     gx, gy = np.zeros(g.n), np.zeros(g.n)
-    S.pc_compute(gx, gy, grid, w_ref)
+    S.pc_compute(gx, gy, pc, panels, g.xs, g.ys, g.zs, d, w_ref)
     qx, qy = np.zeros(g.n), np.zeros(g.n)
-    S.pp_compute(qx, qy, grid, h)
+    S.pp_compute(qx, qy, pp, panels, g.xs, g.ys, g.zs, g.areas, h)
+    S.dropin_release()
     # the oracle on every list entry of 4,000 seeded targets
     tg = np.sort(np.random.default_rng(21).choice(g.n, 4000, replace=False))
     sel = np.zeros(g.n + 1, bool)

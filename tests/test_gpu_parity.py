@@ -62,7 +62,11 @@ def test_accurate_form_matches_oracle_cartesian(name, thresh):
     S, O, g, h, ot, pt, L = _setup(name, thresh, 8)
     ox, oy = O.fast_sum_cart(ot, L, g.xs, g.ys, g.zs, g.areas, h, 8, 8)
     gx, gy = np.zeros(g.n), np.zeros(g.n)
-    S.fast_sum(gx, gy, L, pt, g.xs, g.ys, g.zs, g.areas, h, g.n, 8, form=S.FORM_ACCURATE)
+    S.dropin_config(S.FORM_ACCURATE)
+    try:
+        S.fast_sum(gx, gy, L, pt, g.xs, g.ys, g.zs, g.areas, h, g.n, 8)
+    finally:
+        S.dropin_config(S.FORM_REF)
     assert rel_l2(gx, gy, ox, oy) <= TOL_PARITY
 
 
@@ -102,13 +106,13 @@ def test_mom6_entry_points_match_oracle(ref_compat):
     pt = S.tree_traverse(g.xs, g.ys, g.zs, g.n, thresh)
     grid = S.mom6_grid(pt, pc, pp, g.xs, g.ys, g.zs, g.areas, d, ref_compat=ref_compat)
     w = np.zeros_like(w_ref)
-    S.proxy_source_compute(w, grid, h)
+    grid.proxy_source_compute_host(h, w)
     assert np.linalg.norm(w - w_ref) <= TOL_PARITY * np.linalg.norm(w_ref)
     gx, gy = np.zeros(g.n), np.zeros(g.n)
-    S.pc_compute(gx, gy, grid, w_ref)
+    grid.pc_compute_host(w_ref, gx, gy)
     assert rel_l2(gx, gy, ox, oy) <= TOL_PARITY
     qx, qy = np.zeros(g.n), np.zeros(g.n)
-    S.pp_compute(qx, qy, grid, h)
+    grid.pp_compute_host(h, qx, qy)
     assert rel_l2(qx, qy, px, py) <= TOL_PARITY
 
 

@@ -130,3 +130,36 @@ def test_identical_points_stop_refining():
     zs = np.full(30, 0.8)
     t = S.tree_traverse(xs, ys, zs, 30, 10)
     assert t.info()[2] == 40
+
+
+def test_reference_signature_entry_points_check_their_arguments_on_the_host():
+    """The panels-without-points_inside path rebuilds the tree from the
+    coordinates and compares it with the caller's panels before any device
+    work: matching panels get as far as the device (SAL_ENODEV here, with no
+    GPU), panels of other coordinates are refused with SAL_ETREE."""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    import salgpu as S
+    g, hh = grid_and_ssh("small_3000")
+    ot = O.tree_traverse(g.xs, g.ys, g.zs, 20)
+    L = O.dual_tree_traversal(ot, 0.7, 20)
+    panels = {k: getattr(ot, k) for k in ("level", "is_leaf", "id", "parent", "child", "face", "bounds", "pt_off",
+                                           "pt_idx")}
+    lon, lat = np.zeros(g.n), np.zeros(g.n)
+    args = (lon, lat, L, panels, g.xs, g.ys, g.zs, g.areas, hh[0], g.n, 8)
+    with pytest.raises(S.SalError) as e:
+        S.fast_sum(*args, 3, 3)
+    assert e.value.code == S.SAL_EINVAL
+    for wp in (True, False):
+        with pytest.raises(S.SalError) as e:
+            S.fast_sum(*args, 0, 1, with_points_inside=wp)
+        assert e.value.code == S.SAL_ENODEV
+    xs2 = g.xs.copy()
+    k = int(np.argmax(np.abs(g.xs)))
+    xs2[k], ys2 = g.ys[k], g.ys.copy()
+    ys2[k] = g.xs[k]                               # one point moved to another place on the sphere
+    with pytest.raises(S.SalError) as e:
+        S.fast_sum(lon, lat, L, panels, xs2, ys2, g.zs, g.areas, hh[0], g.n, 8, with_points_inside=False)
+    assert e.value.code == S.SAL_ETREE
+    assert not lon.any() and not lat.any()
