@@ -124,11 +124,49 @@ typedef struct {
     int64_t device_bytes;                            /* resident device memory of the grid */
     double setup_seconds;                            /* plan build + upload */
     int64_t mixed_bytes;                             /* device memory the batched form adds on its first solve */
+    double macs_up_batched, macs_down_batched;       /* the batched form's basis multiply-adds per field: the
+                                                        leaf-level upward and DOWN work of its tree passes (or the
+                                                        direct ones, as macs_up / macs_down, when those are off) */
 } sal_grid_stats;
+
+/* Runtime choices of the batched form's tcgen05 passes (no counterpart in the
+ * reference): the search space of sal_grid_autotune. */
+typedef struct {
+    int32_t chain_ksteps;       /* k-steps (8 sources) an accumulator chain reaches before it is folded into the
+                                   running sums: longer chains fold less often, shorter ones round less (the tensor
+                                   cores accumulate with truncation) */
+    int32_t tree_passes;        /* 1: leaf-level upward pass plus child-to-parent transfers, parent-to-child
+                                   transfers plus one DOWN item per leaf; 0: the direct per-slot passes
+                                   (degrees above 10 always use the direct passes) */
+    int32_t up_chunk;           /* direct upward pass: points per work unit at least */
+    int32_t proxy_unit_kpairs;  /* proxy pass: kernel pairs per work unit, in units of 1024 */
+    int32_t cta_groups;         /* tcgen05 launches: target groups one CTA walks at most */
+    int32_t field_block;        /* fields per block: 64 (tcgen05 passes) or 32 (mma.sync passes) */
+} sal_tune;
 
 /* Flattens the tree and lists into device-resident arrays (once per grid). */
 int sal_grid_create(const sal_tree *t, const sal_grid_desc *desc, sal_grid **out);
 int sal_grid_stats_get(const sal_grid *g, sal_grid_stats *s);
+
+/* The batched form's current choices; setting them re-cuts its plan and
+ * frees its buffers (allocated again by the next batched solve, so the
+ * grid's work on its streams must be finished).  SAL_MODE_DTT grids only. */
+int sal_grid_tune_get(const sal_grid *g, sal_tune *t);
+int sal_grid_tune_set(sal_grid *g, const sal_tune *t);
+
+/* Autotuner of the batched form (no counterpart in the reference).  Times
+ * SAL_FORM_MIXED solves of the caller's nfields device fields (column f at
+ * ssh + f * ld_ssh, caller's order, nfields <= 64) for candidate sal_tune
+ * settings, by coordinate descent from the current setting over each
+ * choice's candidates, with CUDA events on the grid's stream and a 256 MB
+ * L2 flush before each timed solve.  A candidate counts only if the
+ * relative L2 error of its first field, at ntargets evenly spaced points,
+ * against the FP64 direct sum stays <= max_rel_err.  The fastest is set on
+ * the grid and returned in *best; *ms_best and *ms_start (may be NULL)
+ * receive its time and the starting setting's.  Synchronous; allocates
+ * scratch for the check and the flush. */
+int sal_grid_autotune(sal_grid *g, const double *ssh, int32_t nfields, int64_t ld_ssh, int32_t ntargets,
+                      double max_rel_err, sal_tune *best, double *ms_best, double *ms_start);
 
 /* Waits for the grid's work on stream (NULL: the grid's own stream) and
  * returns SAL_ETIMEOUT if a device-side staging wait gave up since the last

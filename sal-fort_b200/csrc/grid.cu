@@ -2,6 +2,8 @@
 #include <cuda_runtime.h>
 
 #include <chrono>
+#include <cmath>
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -30,6 +32,7 @@ struct DBuf {
 struct GridImpl {
     int dev = 0;
     Plan plan;
+    Tree tree;                        // kept to re-cut the tcgen05 plan (sal_grid_tune)
     cudaStream_t stream = nullptr;
     int64_t bytes = 0;
     double setup_seconds = 0;
@@ -78,7 +81,11 @@ struct GridImpl {
     int nsm = 0;
     Item *mix_leaf_items = nullptr, *mix_proxy_items = nullptr;
     double *tgt_nodes = nullptr;
+    // tcgen05 plan (tree passes, its own proxy units)
+    int32_t *m2m_tasks = nullptr, *l2l_tasks = nullptr, *tc_proxy_unit_beg = nullptr;
+    double *tc_up_nodes = nullptr, *tc_down_nodes = nullptr;
     int64_t mix_bytes = 0;
+    std::vector<std::pair<void **, size_t>> mix_allocs;   // the batched form's buffers (release_mixed frees them)
     // staging for the *_host entry points
     double *h_ssh = nullptr, *h_ox = nullptr, *h_oy = nullptr;  // device
     double *hb_ssh = nullptr, *hb_ox = nullptr, *hb_oy = nullptr;  // device, batched
@@ -174,6 +181,47 @@ static int dupload(GridImpl &g, T **p, const T *src, size_t count) {
     return SAL_OK;
 }
 
+// dalloc / dupload of a batched-form buffer, recorded for release_mixed.
+template <class T>
+static int malloc_mix(GridImpl &g, T **p, size_t count) {
+    int rc = dalloc(g, p, count);
+    if (!rc && *p) g.mix_allocs.push_back({(void **)p, count * sizeof(T)});
+    return rc;
+}
+template <class T>
+static int upload_mix(GridImpl &g, T **p, const std::vector<T> &v) {
+    int rc = malloc_mix(g, p, v.size());
+    if (rc || v.empty()) return rc;
+    CK(cudaMemcpy(*p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+    return SAL_OK;
+}
+
+// Frees every batched-form buffer once the grid's stream is idle; the next
+// batched solve allocates them again for the current tcgen05 plan.
+static int release_mixed(GridImpl &g) {
+    CK(cudaStreamSynchronize(g.stream));
+    for (auto &e : g.mix_allocs) {
+        void *ptr = *e.first;
+        for (size_t i = 0; i < g.allocs.size(); ++i)
+            if (g.allocs[i] == ptr) {
+                g.allocs.erase(g.allocs.begin() + (std::ptrdiff_t)i);
+                break;
+            }
+        cudaFree(ptr);
+        g.bytes -= (int64_t)e.second;
+        *e.first = nullptr;
+    }
+    g.mix_allocs.clear();
+    g.FT = 0;
+    g.mix_bytes = 0;
+    // captured graphs name the freed buffers
+    std::lock_guard<std::mutex> lk(g.graph_mu);
+    for (auto &e : g.graphs) cudaGraphExecDestroy(e.exec);
+    g.graphs.clear();
+    g.seen.clear();
+    return SAL_OK;
+}
+
 static void grid_free(GridImpl &g) {
     if (g.dev >= 0) cudaSetDevice(g.dev);
     for (auto &e : g.ev)
@@ -219,6 +267,7 @@ extern "C" int sal_grid_create(const sal_tree *t_, const sal_grid_desc *d, sal_g
     GridImpl &g = G->g;
     g.dev = d->device;
     g.max_fields = d->max_fields;
+    if (d->mode == SAL_MODE_DTT) g.tree = t;
     std::string err;
     if (!plan_build(t, d->interp_degree, d->mode, d->list, d->list_count, d->pc_list, d->pc_count, d->pp_list,
                     d->pp_count, &g.plan, &err)) {
@@ -328,6 +377,8 @@ extern "C" int sal_grid_stats_get(const sal_grid *G, sal_grid_stats *s) {
     s->macs_down = pl.macs_down;
     s->device_bytes = g.bytes;
     s->setup_seconds = g.setup_seconds;
+    s->macs_up_batched = pl.tc_items.empty() ? pl.macs_up : pl.tc_macs_up;
+    s->macs_down_batched = pl.tc_items.empty() ? pl.macs_down : pl.tc_macs_down;
     {
         const int64_t FT = g.FT ? g.FT : (g.max_fields <= 32 ? 32 : 64), P = pl.P;
         s->mixed_bytes = g.FT ? g.mix_bytes
@@ -418,51 +469,62 @@ static int ensure_mixed(GridImpl &g, int FT) {
     const Plan &pl = g.plan;
     const size_t P = (size_t)pl.P, n = (size_t)pl.n;
     const int64_t before = g.bytes;
+    const bool tc = FT == 64 && !pl.tc_items.empty();
+    // proxy-weight rows: source slots (and, in the tree passes, the other
+    // panels below them); potential rows: target slots (and the panels below)
+    const size_t nw = tc ? (size_t)pl.n_wslots : (size_t)g.nsrc, ndn = tc ? (size_t)pl.n_dslots : (size_t)g.ntgt;
+    const size_t nunits_p = std::max((size_t)g.nproxy_units, (size_t)pl.tc_nproxy_units);
     int rc = SAL_OK;
-    if (!rc) rc = dalloc(g, &g.wF, (n + (size_t)g.nsrc * P) * FT);
-    if (!rc) rc = dalloc(g, &g.phiF, (size_t)g.ntgt * 3 * P * FT);
-    if (!rc) rc = dalloc(g, &g.mix_up_partial, (size_t)g.nup * P * FT);
-    if (!rc) rc = dalloc(g, &g.mix_proxy_partial, (size_t)g.nproxy_units * 3 * P * FT);
+    if (!rc) rc = malloc_mix(g, &g.wF, (n + nw * P) * FT);
+    if (!rc) rc = malloc_mix(g, &g.phiF, ndn * 3 * P * FT);
+    if (!rc) rc = malloc_mix(g, &g.mix_up_partial, (size_t)g.nup * P * FT);
+    if (!rc) rc = malloc_mix(g, &g.mix_proxy_partial, nunits_p * 3 * P * FT);
     if (!rc) {
         std::vector<int32_t> ip(n);
         for (size_t p = 0; p < n; ++p) ip[(size_t)pl.perm[p]] = (int32_t)p;
-        rc = dupload(g, &g.iperm, ip.data(), ip.size());
+        rc = upload_mix(g, &g.iperm, ip);
     }
-    if (!rc) rc = dupload(g, &g.mix_leaf_groups, pl.mix_leaf_groups.data(), pl.mix_leaf_groups.size());
-    if (!rc) rc = dupload(g, &g.mix_leaf_items, pl.mix_leaf_items.data(), pl.mix_leaf_items.size());
-    if (!rc) rc = dupload(g, &g.mix_proxy_groups, pl.mix_proxy_groups.data(), pl.mix_proxy_groups.size());
-    if (!rc) rc = dupload(g, &g.mix_proxy_items, pl.mix_proxy_items.data(), pl.mix_proxy_items.size());
-    if (!rc) rc = dupload(g, &g.mix_up_groups, pl.mix_up_groups.data(), pl.mix_up_groups.size());
-    if (!rc && FT == 64 && !pl.tc_items.empty()) {
-        // tcgen05 leaf pass: items, split weight store, per-row source
-        // coordinates and the per-point self pairs
-        rc = dupload(g, &g.tc_leaf_groups, pl.tc_leaf_groups.data(), pl.tc_leaf_groups.size());
-        if (!rc) rc = dupload(g, &g.tc_items, pl.tc_items.data(), pl.tc_items.size());
-        if (!rc) rc = dupload(g, &g.tc_proxy_groups, pl.tc_proxy_groups.data(), pl.tc_proxy_groups.size());
-        if (!rc) rc = dupload(g, &g.tc_proxy_items, pl.tc_proxy_items.data(), pl.tc_proxy_items.size());
-        if (!rc) rc = dupload(g, &g.tc_up_groups, pl.tc_up_groups.data(), pl.tc_up_groups.size());
-        if (!rc) rc = dupload(g, &g.tc_up_items, pl.tc_up_items.data(), pl.tc_up_items.size());
-        if (!rc) rc = dupload(g, &g.tc_up_unit_beg, pl.tc_up_unit_beg.data(), pl.tc_up_unit_beg.size());
-        const int64_t nbk = (int64_t)pl.tc_bas.size() / 3, nunits = pl.tc_up_unit_beg.empty() ? 0 : pl.tc_up_unit_beg.back();
-        if (!rc) rc = dalloc(g, &g.tc_up_partial, (size_t)nunits * P * FT);
-        if (!rc) rc = dalloc(g, &g.basis, (size_t)nbk * 16 * (pl.d + 1));
+    if (!rc) rc = upload_mix(g, &g.mix_leaf_groups, pl.mix_leaf_groups);
+    if (!rc) rc = upload_mix(g, &g.mix_leaf_items, pl.mix_leaf_items);
+    if (!rc) rc = upload_mix(g, &g.mix_proxy_groups, pl.mix_proxy_groups);
+    if (!rc) rc = upload_mix(g, &g.mix_proxy_items, pl.mix_proxy_items);
+    if (!rc) rc = upload_mix(g, &g.mix_up_groups, pl.mix_up_groups);
+    if (!rc && tc) {
+        // tcgen05 passes: items, split weight store, per-row source
+        // coordinates, the per-point self pairs and the tree transfers
+        rc = upload_mix(g, &g.tc_leaf_groups, pl.tc_leaf_groups);
+        if (!rc) rc = upload_mix(g, &g.tc_items, pl.tc_items);
+        if (!rc) rc = upload_mix(g, &g.tc_proxy_groups, pl.tc_proxy_groups);
+        if (!rc) rc = upload_mix(g, &g.tc_proxy_items, pl.tc_proxy_items);
+        if (!rc) rc = upload_mix(g, &g.tc_proxy_unit_beg, pl.tc_proxy_unit_beg);
+        if (!rc) rc = upload_mix(g, &g.tc_up_groups, pl.tc_up_groups);
+        if (!rc) rc = upload_mix(g, &g.tc_up_items, pl.tc_up_items);
+        if (!rc) rc = upload_mix(g, &g.tc_up_unit_beg, pl.tc_up_unit_beg);
+        if (!rc) rc = upload_mix(g, &g.tc_up_nodes, pl.tc_up_nodes);
+        if (!rc) rc = upload_mix(g, &g.tc_down_nodes, pl.tc_down_nodes);
+        if (!rc) rc = upload_mix(g, &g.m2m_tasks, pl.m2m_tasks);
+        if (!rc) rc = upload_mix(g, &g.l2l_tasks, pl.l2l_tasks);
+        const int64_t nbk = (int64_t)pl.tc_bas.size() / 3,
+                      nunits = pl.tc_up_unit_beg.empty() ? 0 : pl.tc_up_unit_beg.back();
+        if (!rc) rc = malloc_mix(g, &g.tc_up_partial, (size_t)nunits * P * FT);
+        if (!rc) rc = malloc_mix(g, &g.basis, (size_t)nbk * 16 * (pl.d + 1));
         if (!rc && nbk > 0) {
-            // the basis store, once per grid
+            // the basis store, once per plan
             int32_t *bas = nullptr;
             CK(cudaMalloc((void **)&bas, pl.tc_bas.size() * sizeof(int32_t)));
             cudaError_t e = cudaMemcpy(bas, pl.tc_bas.data(), pl.tc_bas.size() * sizeof(int32_t), cudaMemcpyHostToDevice);
             if (e == cudaSuccess) {
-                mix::launch_basis_store(bas, nbk, g.xieta, g.src_nodes, pl.d + 1, g.basis, g.stream);
+                mix::launch_basis_store(bas, nbk, g.xieta, g.tc_up_nodes, pl.d + 1, g.basis, g.stream);
                 e = cudaStreamSynchronize(g.stream);
             }
             cudaFree(bas);
             if (e != cudaSuccess) return set_error(SAL_ECUDA, std::string("basis store: ") + cudaGetErrorString(e));
         }
-        if (!rc) rc = dupload(g, &g.bsrc, pl.bsrc.data(), pl.bsrc.size());
-        if (!rc) rc = dalloc(g, &g.bstore, pl.bsrc.size() * 2 * (size_t)FT);
-        if (!rc) rc = dalloc(g, &g.sloc, n + (size_t)g.nsrc * P);
-        if (!rc) rc = dalloc(g, &g.selfk, n);
-        if (!rc) rc = dalloc(g, &g.sxyz, (size_t)pl.tc_src_ksteps * 24);
+        if (!rc) rc = upload_mix(g, &g.bsrc, pl.bsrc);
+        if (!rc) rc = malloc_mix(g, &g.bstore, pl.bsrc.size() * 2 * (size_t)FT);
+        if (!rc) rc = malloc_mix(g, &g.sloc, n + (size_t)g.nsrc * P);
+        if (!rc) rc = malloc_mix(g, &g.selfk, n);
+        if (!rc) rc = malloc_mix(g, &g.sxyz, (size_t)pl.tc_src_ksteps * 24);
         if (!rc) {
             const size_t nr = pl.sloc_ranges.size() / 2;
             std::vector<int2> ranges(nr);
@@ -489,7 +551,10 @@ static int ensure_mixed(GridImpl &g, int FT) {
         }
         if (!rc) CK(cudaDeviceGetAttribute(&g.nsm, cudaDevAttrMultiProcessorCount, g.dev));
     }
-    if (rc) return rc;
+    if (rc) {
+        release_mixed(g);
+        return rc;
+    }
     g.FT = FT;
     g.mix_bytes = g.bytes - before;
     return SAL_OK;
@@ -519,6 +584,8 @@ static void solve_mixed_block(GridImpl &g, const double *ssh, int64_t ld_ssh, in
     a.ld_out = ld_out;
     a.f0 = f0;
     a.nf = nf;
+    const bool tree = g.bstore && pl.tc_opt.tree_passes;
+    const int cg = pl.tc_opt.cta_groups;
     if (g.bstore) {
         // 64-field blocks, tcgen05: the points' rows of the split weight store,
         // then the upward pass; then the proxies' rows
@@ -532,10 +599,17 @@ static void solve_mixed_block(GridImpl &g, const double *ssh, int64_t ld_ssh, in
             u.basis = g.basis;
             u.d = pl.d;
             u.P = P;
-            u.partial = g.tc_up_partial;
-            mix::launch_tc_upward(u, g.nsm, g.err, st);
-            mix::launch_finalize_mix(g.tc_up_unit_beg, g.tc_up_partial, g.nsrc, P, FT, g.wF + (size_t)n * FT, st);
+            // tree passes: every unit is one leaf, written straight to its
+            // proxy-weight rows; direct passes: unit partials, summed per slot
+            u.partial = tree ? g.wF + (size_t)n * FT : g.tc_up_partial;
+            mix::launch_tc_upward(u, g.nsm, cg, g.err, st);
+            if (!tree)
+                mix::launch_finalize_mix(g.tc_up_unit_beg, g.tc_up_partial, g.nsrc, P, FT, g.wF + (size_t)n * FT, st);
         }
+        if (tree)
+            for (size_t l = 0; l + 1 < pl.m2m_level_beg.size(); ++l)
+                mix::launch_m2m(g.m2m_tasks + 5 * (size_t)pl.m2m_level_beg[l], pl.m2m_level_beg[l + 1] - pl.m2m_level_beg[l],
+                                g.tc_up_nodes, pl.d + 1, g.wF + (size_t)n * FT, st);
         mix::launch_split_store(g.bsrc, pl.tc_pt_ksteps, pl.tc_src_ksteps, g.wF, g.phiF, g.bstore, st);
     } else if (!pl.mix_up_groups.empty()) {
         mix::MixArgs u = a;
@@ -558,8 +632,12 @@ static void solve_mixed_block(GridImpl &g, const double *ssh, int64_t ld_ssh, in
         p.d = pl.d;
         p.P = P;
         p.partial = g.mix_proxy_partial;
-        mix::launch_tc_proxy(p, g.nsm, g.err, st);
-        mix::launch_finalize_mix(g.proxy_unit_beg, g.mix_proxy_partial, g.ntgt, 3 * P, FT, g.phiF, st);
+        mix::launch_tc_proxy(p, g.nsm, cg, g.err, st);
+        mix::launch_finalize_mix(g.tc_proxy_unit_beg, g.mix_proxy_partial, g.ntgt, 3 * P, FT, g.phiF, st);
+        if (tree)
+            for (size_t l = 0; l + 1 < pl.l2l_level_beg.size(); ++l)
+                mix::launch_l2l(g.l2l_tasks + 3 * (size_t)pl.l2l_level_beg[l], pl.l2l_level_beg[l + 1] - pl.l2l_level_beg[l],
+                                g.tc_down_nodes, pl.d + 1, g.phiF, st);
     } else if (!pl.mix_proxy_groups.empty()) {
         mix::MixArgs q = a;
         q.groups = g.mix_proxy_groups;
@@ -585,7 +663,7 @@ static void solve_mixed_block(GridImpl &g, const double *ssh, int64_t ld_ssh, in
         t.bstore = g.bstore;
         t.tgt = g.pool;
         t.xieta = g.xieta;
-        t.tgt_nodes = g.tgt_nodes;
+        t.tgt_nodes = g.tc_down_nodes;
         t.selfk = g.selfk;
         t.wF = g.wF;
         t.perm = g.perm;
@@ -596,7 +674,7 @@ static void solve_mixed_block(GridImpl &g, const double *ssh, int64_t ld_ssh, in
         t.ld_out = ld_out;
         t.f0 = f0;
         t.nf = nf;
-        mix::launch_tc_leaf(t, g.nsm, g.err, st);
+        mix::launch_tc_leaf(t, g.nsm, cg, g.err, st);
     } else {
         a.groups = g.mix_leaf_groups;
         mix::launch_mix(0, FT, a, (int)pl.mix_leaf_groups.size(), st);
@@ -710,6 +788,208 @@ extern "C" int sal_solve(sal_grid *G, const double *ssh, int32_t nf, int64_t ld_
                    g.plan.mode == SAL_MODE_DTT ? form : SAL_FORM_REF, 7, true, st);
     CK(cudaGetLastError());
     return SAL_OK;
+}
+
+// ------------------------------------------------------------------ tuning of the batched form
+static sal_tune tune_of(const GridImpl &g) {
+    const TcOptions &o = g.plan.tc_opt;
+    sal_tune t{};
+    t.chain_ksteps = o.chain_ksteps;
+    t.tree_passes = o.tree_passes;
+    t.up_chunk = o.up_chunk;
+    t.proxy_unit_kpairs = o.proxy_unit_kpairs;
+    t.cta_groups = o.cta_groups;
+    t.field_block = g.FT ? g.FT : (g.max_fields <= 32 ? 32 : 64);
+    return t;
+}
+
+static int apply_tune(GridImpl &g, const sal_tune &t) {
+    if (t.field_block != 32 && t.field_block != 64) return set_error(SAL_EINVAL, "field_block must be 32 or 64");
+    TcOptions o;
+    o.chain_ksteps = t.chain_ksteps;
+    o.tree_passes = t.tree_passes ? 1 : 0;
+    o.up_chunk = t.up_chunk;
+    o.proxy_unit_kpairs = t.proxy_unit_kpairs;
+    o.cta_groups = t.cta_groups;
+    const TcOptions &c = g.plan.tc_opt;
+    const bool same_plan = o.chain_ksteps == c.chain_ksteps && o.tree_passes == c.tree_passes &&
+                           o.up_chunk == c.up_chunk && o.proxy_unit_kpairs == c.proxy_unit_kpairs;
+    const int cur_block = g.FT ? g.FT : (g.max_fields <= 32 ? 32 : 64);
+    if (same_plan && t.field_block == cur_block) {
+        if (o.cta_groups < 1) return set_error(SAL_EINVAL, "tcgen05 options must be positive");
+        g.plan.tc_opt.cta_groups = o.cta_groups;
+        return SAL_OK;
+    }
+    int rc = release_mixed(g);
+    if (rc) return rc;
+    g.max_fields = t.field_block;
+    if (!same_plan) {
+        std::string err;
+        if (!plan_build_tc(g.tree, &g.plan, o, &err)) return set_error(SAL_EINVAL, err);
+    } else {
+        g.plan.tc_opt.cta_groups = o.cta_groups;
+    }
+    return SAL_OK;
+}
+
+extern "C" int sal_grid_tune_get(const sal_grid *G, sal_tune *t) {
+    if (!G || !t) return set_error(SAL_EINVAL, "null argument");
+    if (G->g.plan.mode != SAL_MODE_DTT) return set_error(SAL_EINVAL, "the batched form needs a SAL_MODE_DTT grid");
+    *t = tune_of(G->g);
+    return SAL_OK;
+}
+
+extern "C" int sal_grid_tune_set(sal_grid *G, const sal_tune *t) {
+    if (!G || !t) return set_error(SAL_EINVAL, "null argument");
+    GridImpl &g = G->g;
+    if (g.plan.mode != SAL_MODE_DTT) return set_error(SAL_EINVAL, "the batched form needs a SAL_MODE_DTT grid");
+    CK(cudaSetDevice(g.dev));
+    return apply_tune(g, *t);
+}
+
+static int finish(GridImpl &g, cudaStream_t st);
+
+extern "C" int sal_grid_autotune(sal_grid *G, const double *ssh, int32_t nf, int64_t ld, int32_t ntargets,
+                                 double max_rel_err, sal_tune *best, double *ms_best, double *ms_start) {
+    if (!G || !ssh || !best) return set_error(SAL_EINVAL, "null argument");
+    GridImpl &g = G->g;
+    const Plan &pl = g.plan;
+    const int64_t n = pl.n;
+    if (pl.mode != SAL_MODE_DTT) return set_error(SAL_EINVAL, "the batched form needs a SAL_MODE_DTT grid");
+    if (nf < 1 || nf > 64) return set_error(SAL_EINVAL, "nfields must be in 1..64");
+    if (nf > 1 && ld < n) return set_error(SAL_EINVAL, "leading dimension < point_count");
+    if (ntargets < 1 || ntargets > n || ntargets > (1 << 20)) return set_error(SAL_EINVAL, "ntargets out of range");
+    if (!(max_rel_err > 0)) return set_error(SAL_EINVAL, "max_rel_err must be positive");
+    CK(cudaSetDevice(g.dev));
+    cudaStream_t st = g.stream;
+    // scratch: outputs, the pool-order sources of field 0, the FP64 direct
+    // sum at the targets, an L2 flush buffer
+    const int nt = ntargets;
+    const int nch = dev::direct_chunks((int)n);
+    const size_t flush_bytes = 256u << 20;
+    double *out = nullptr, *src = nullptr, *ref = nullptr, *dscr = nullptr;
+    double4 *pool = nullptr;
+    int32_t *tg = nullptr;
+    void *flush = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    std::vector<int32_t> tpos(nt), tidx(nt);
+    std::vector<double> rx(nt), ry(nt), ox(n), oy(n);
+    auto cleanup = [&]() {
+        for (void *p : {(void *)out, (void *)src, (void *)ref, (void *)dscr, (void *)pool, (void *)tg, flush})
+            if (p) cudaFree(p);
+        if (e0) cudaEventDestroy(e0);
+        if (e1) cudaEventDestroy(e1);
+    };
+#define TCK(call)                                                                                 \
+    do {                                                                                          \
+        cudaError_t e_ = (call);                                                                  \
+        if (e_ != cudaSuccess) {                                                                  \
+            cleanup();                                                                            \
+            return set_error(SAL_ECUDA, std::string(#call) + ": " + cudaGetErrorString(e_));     \
+        }                                                                                         \
+    } while (0)
+    TCK(cudaMalloc((void **)&out, 2 * (size_t)n * nf * sizeof(double)));
+    TCK(cudaMalloc((void **)&src, 4 * (size_t)n * sizeof(double)));
+    TCK(cudaMalloc((void **)&ref, 2 * (size_t)nt * sizeof(double)));
+    TCK(cudaMalloc((void **)&dscr, (size_t)nch * nt * 2 * sizeof(double)));
+    TCK(cudaMalloc((void **)&pool, (size_t)n * sizeof(double4)));
+    TCK(cudaMalloc((void **)&tg, (size_t)nt * sizeof(int32_t)));
+    TCK(cudaMalloc(&flush, flush_bytes));
+    TCK(cudaEventCreate(&e0));
+    TCK(cudaEventCreate(&e1));
+    // evenly spaced caller indices; the direct sum runs over pool-order sources
+    std::vector<int32_t> iperm(n);
+    for (int64_t p = 0; p < n; ++p) iperm[pl.perm[p]] = (int32_t)p;
+    for (int k = 0; k < nt; ++k) {
+        tidx[k] = (int32_t)(((int64_t)k * n) / nt);
+        tpos[k] = iperm[tidx[k]];
+    }
+    TCK(cudaMemcpy(tg, tpos.data(), nt * sizeof(int32_t), cudaMemcpyHostToDevice));
+    dev::launch_prep(g.xyz, g.area, ssh, g.perm, (int)n, pool, st);
+    for (int c = 0; c < 4; ++c)
+        TCK(cudaMemcpy2DAsync(src + (size_t)c * n, sizeof(double), (const double *)pool + c, sizeof(double4), sizeof(double),
+                              (size_t)n, cudaMemcpyDeviceToDevice, st));
+    dev::launch_direct(src, src + n, src + 2 * n, src + 3 * n, (int)n, tg, nt, ref, ref + nt, dscr, nch, st);
+    TCK(cudaMemcpyAsync(rx.data(), ref, nt * sizeof(double), cudaMemcpyDeviceToHost, st));
+    TCK(cudaMemcpyAsync(ry.data(), ref + nt, nt * sizeof(double), cudaMemcpyDeviceToHost, st));
+    TCK(cudaStreamSynchronize(st));
+    double den = 0;
+    for (int k = 0; k < nt; ++k) den += rx[k] * rx[k] + ry[k] * ry[k];
+    double *oxd = out, *oyd = out + (size_t)n * nf;
+    // time and check one setting: -1 if it failed to run
+    auto evaluate = [&](const sal_tune &t, double *ms, double *err) -> int {
+        int rc = apply_tune(g, t);
+        if (rc) return rc;
+        rc = sal_solve(G, ssh, nf, ld, oxd, oyd, n, SAL_FORM_MIXED, st);
+        if (rc) return rc;
+        rc = finish(g, st);
+        if (rc) return rc;
+        cudaMemcpy(ox.data(), oxd, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost);
+        cudaMemcpy(oy.data(), oyd, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost);
+        double num = 0;
+        for (int k = 0; k < nt; ++k) {
+            const double dx = ox[tidx[k]] - rx[k], dy = oy[tidx[k]] - ry[k];
+            num += dx * dx + dy * dy;
+        }
+        *err = den > 0 ? std::sqrt(num / den) : std::sqrt(num);
+        double tmin = 1e30;
+        for (int r = 0; r < 3; ++r) {
+            cudaMemsetAsync(flush, r & 0xff, flush_bytes, st);
+            cudaEventRecord(e0, st);
+            rc = sal_solve(G, ssh, nf, ld, oxd, oyd, n, SAL_FORM_MIXED, st);
+            if (rc) return rc;
+            cudaEventRecord(e1, st);
+            cudaEventSynchronize(e1);
+            float t_ms = 0;
+            cudaEventElapsedTime(&t_ms, e0, e1);
+            tmin = std::min(tmin, (double)t_ms);
+        }
+        *ms = tmin;
+        return finish(g, st);
+    };
+    sal_tune cur = tune_of(g), top = cur;
+    double top_ms = 0, top_err = 0;
+    int rc = evaluate(cur, &top_ms, &top_err);
+    if (rc) { cleanup(); return rc; }
+    const double start_ms = top_ms;
+    const bool start_ok = top_err <= max_rel_err;
+    if (!start_ok) top_ms = 1e30;   // any passing setting beats a failing start
+    // coordinate descent: each choice's candidates with the others held at
+    // the best so far
+    struct Axis { int32_t sal_tune::*field; std::vector<int32_t> values; };
+    const std::vector<Axis> axes = {
+        {&sal_tune::tree_passes, {1, 0}},
+        {&sal_tune::chain_ksteps, {8, 16, 32, 64}},
+        {&sal_tune::cta_groups, {1, 2, 4}},
+        {&sal_tune::proxy_unit_kpairs, {324, 648, 1296}},
+        {&sal_tune::up_chunk, {2048, 4096, 8192}},
+        {&sal_tune::field_block, {64, 32}},
+    };
+    for (const Axis &ax : axes) {
+        if (ax.field == &sal_tune::up_chunk && top.tree_passes) continue;   // only the direct upward pass uses it
+        for (int32_t v : ax.values) {
+            if (top.*(ax.field) == v) continue;
+            sal_tune t = top;
+            t.*(ax.field) = v;
+            double ms = 0, err = 0;
+            rc = evaluate(t, &ms, &err);
+            if (rc) { cleanup(); return rc; }
+            if (err <= max_rel_err && ms < top_ms) { top = t; top_ms = ms; top_err = err; }
+        }
+    }
+    if (top_ms >= 1e30) {
+        apply_tune(g, cur);
+        cleanup();
+        return set_error(SAL_EINVAL, "no setting meets max_rel_err");
+    }
+    rc = apply_tune(g, top);
+    cleanup();
+    if (rc) return rc;
+    *best = top;
+    if (ms_best) *ms_best = top_ms;
+    if (ms_start) *ms_start = start_ms;
+    return SAL_OK;
+#undef TCK
 }
 
 // Synchronises the grid's work on `stream` and reports a kernel time-out.

@@ -67,9 +67,11 @@ struct TcArgs {
     float *partial;           // proxy / upward pass: per-unit rows (P x components x 64 fields)
     const float *basis;       // upward pass: BLI factors per basis k-step
 };
-void launch_tc_leaf(const TcArgs &a, int nsm, int *err, cudaStream_t st);
-void launch_tc_proxy(const TcArgs &a, int nsm, int *err, cudaStream_t st);
-void launch_tc_upward(const TcArgs &a, int nsm, int *err, cudaStream_t st);
+// cta_groups: groups one CTA walks at most (the grid has every SM busy
+// otherwise)
+void launch_tc_leaf(const TcArgs &a, int nsm, int cta_groups, int *err, cudaStream_t st);
+void launch_tc_proxy(const TcArgs &a, int nsm, int cta_groups, int *err, cudaStream_t st);
+void launch_tc_upward(const TcArgs &a, int nsm, int cta_groups, int *err, cudaStream_t st);
 void launch_basis_store(const int32_t *bas, int64_t nbk, const double2 *xieta, const double *src_nodes, int n,
                         float *basis, cudaStream_t st);
 size_t tc_smem_bytes();
@@ -79,6 +81,9 @@ void launch_source_local(const double4 *pool, const int2 *ranges, const double4 
                          cudaStream_t st);
 void launch_self_pair(const double4 *pool, int n, double2 *selfk, cudaStream_t st);
 void launch_source_ksteps(const int32_t *bsrc, int64_t nks, const float4 *sloc, float *sxyz, cudaStream_t st);
+// tree transfers (transfer.cu): one launch per tree level
+void launch_m2m(const int32_t *tasks, int ntasks, const double *nodes, int n, float *w, cudaStream_t st);
+void launch_l2l(const int32_t *tasks, int ntasks, const double *nodes, int n, float *phi, cudaStream_t st);
 
 }  // namespace mix
 }  // namespace sal

@@ -28,7 +28,7 @@
 namespace sal {
 
 static constexpr int kUpChunk = 4096;          // points per upward unit
-static constexpr double kProxyUnitPairs = 81.0 * 8192.0;  // pair budget of one proxy work unit
+static constexpr double kProxyUnitPairs = 81.0 * 8192.0;  // pair budget of one proxy work unit (FP64 pass)
 
 static void panel_proxies(const Panel &q, int d, double *xyz, double *nodes, double *box) {
     int n = d + 1;
@@ -260,8 +260,10 @@ bool plan_build(const Tree &t, int d, int mode, const int32_t *list, int64_t nli
         pl->proxy_unit_beg.assign(ntgt + 1, 0);
         std::vector<Group> units;
         std::vector<double> ucost;
+        pl->proxy_slot_items.assign(ntgt + 1, 0);
         for (int32_t s = 0; s < ntgt; ++s) {
             pl->proxy_unit_beg[s] = (int32_t)units.size();
+            pl->proxy_slot_items[s] = (int32_t)pl->proxy_items.size();
             const auto &v = titems[s];
             size_t i = 0;
             while (i < v.size()) {
@@ -281,6 +283,7 @@ bool plan_build(const Tree &t, int d, int mode, const int32_t *list, int64_t nli
             }
         }
         pl->proxy_unit_beg[ntgt] = (int32_t)units.size();
+        pl->proxy_slot_items[ntgt] = (int32_t)pl->proxy_items.size();
         std::vector<int32_t> ord(units.size());
         std::iota(ord.begin(), ord.end(), 0);
         std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) { return ucost[a] > ucost[b]; });
@@ -344,12 +347,124 @@ bool plan_build(const Tree &t, int d, int mode, const int32_t *list, int64_t nli
                 }
         }
     }
-    // ---------------------------------------------------------------- tcgen05 leaf pass
-    // The split weight store holds every source row of the leaf pass once, as
-    // TF32 hi/lo tiles per k-step of 8 rows: each leaf's points, then each
-    // source slot's P proxies, then each target slot's 3P potential rows, every
-    // range padded with zero rows to a multiple of 8 so that each item starts
-    // on a k-step boundary and its padding columns meet zero weights.
+    if (dtt && !plan_build_tc(t, pl, TcOptions{}, err)) return false;
+    // ---------------------------------------------------------------- point data in pool order
+    pl->pxi.resize(n); pl->peta.resize(n);
+    for (int32_t p = 0; p < n; ++p) { pl->pxi[p] = t.xi[t.order[p]]; pl->peta[p] = t.eta[t.order[p]]; }
+    return true;
+}
+
+// ---------------------------------------------------------------- tcgen05 passes
+// The split weight store holds every source row of the leaf pass once, as
+// TF32 hi/lo tiles per k-step of 8 rows: each leaf's points, then each source
+// slot's P proxies, then the potential rows (3P per target slot in the direct
+// passes, per leaf under a target slot in the tree passes), every range padded
+// with zero rows to a multiple of 8 so that each item starts on a k-step
+// boundary and its padding columns meet zero weights.
+//
+// Tree passes (opt.tree_passes).  Upward: the weights of every leaf below a
+// source slot come from its own points (one tcgen05 work unit per leaf), and
+// every refined panel below a source slot sums its children's weights moved
+// onto its own Chebyshev nodes (child-to-parent BLI transfer, exact for the
+// degree-d polynomials both grids reproduce), level by level from the
+// deepest.  Downward: every panel below a target slot adds its parent's
+// potentials interpolated at its own nodes (parent-to-child transfer), level
+// by level from the top, so a leaf needs one DOWN item (its own potentials)
+// instead of one per target slot above it.  The FP64 forms keep the
+// reference's direct passes.
+bool plan_build_tc(const Tree &t, Plan *pl, const TcOptions &opt, std::string *err) {
+    const int n = t.n, np = (int)t.p.size(), d = pl->d, nd = d + 1, P = pl->P;
+    const int32_t nsrc = (int32_t)pl->src_slot_panel.size(), ntgt = (int32_t)pl->tgt_slot_panel.size();
+    if (opt.chain_ksteps < 1 || opt.up_chunk < 1 || opt.proxy_unit_kpairs < 1 || opt.cta_groups < 1) {
+        *err = "tcgen05 options must be positive";
+        return false;
+    }
+    pl->tc_opt = opt;
+    if (d > kMaxTreeDegree) pl->tc_opt.tree_passes = 0;   // the transfer tiles fit shared memory up to kMaxTreeDegree
+    std::vector<int32_t> leaves;
+    for (int k = 0; k < np; ++k)
+        if (t.p[k].is_leaf && t.p[k].count() > 0) leaves.push_back(k);
+    std::sort(leaves.begin(), leaves.end(), [&](int a, int b) { return t.p[a].begin < t.p[b].begin; });
+    std::vector<int64_t> leaf_begin(leaves.size());
+    for (size_t i = 0; i < leaves.size(); ++i) leaf_begin[i] = t.p[leaves[i]].begin;
+    auto leaf_range = [&](int k, int32_t *lb, int32_t *le) {
+        const Panel &q = t.p[k];
+        *lb = (int32_t)(std::lower_bound(leaf_begin.begin(), leaf_begin.end(), q.begin) - leaf_begin.begin());
+        *le = (int32_t)(std::lower_bound(leaf_begin.begin(), leaf_begin.end(), q.end) - leaf_begin.begin());
+    };
+    std::vector<int32_t> leaf_of_pos(n, -1);
+    for (size_t i = 0; i < leaves.size(); ++i)
+        for (int64_t q = t.p[leaves[i]].begin; q < t.p[leaves[i]].end; ++q) leaf_of_pos[q] = (int32_t)i;
+    std::vector<int32_t> src_slot(np, -1), tgt_slot(np, -1);
+    for (int32_t s = 0; s < nsrc; ++s) src_slot[pl->src_slot_panel[s]] = s;
+    for (int32_t s = 0; s < ntgt; ++s) tgt_slot[pl->tgt_slot_panel[s]] = s;
+    const bool tree = pl->tc_opt.tree_passes != 0;
+
+    // ---- slots of the tree passes: panels with points below a source
+    // (target) slot, BFS order is parents before children
+    std::vector<int32_t> wslot(np, -1), dslot(np, -1);
+    int32_t nw = nsrc, ndn = ntgt;
+    std::vector<int32_t> wpanel(pl->src_slot_panel), dpanel(pl->tgt_slot_panel);
+    for (int32_t s = 0; s < nsrc; ++s) wslot[pl->src_slot_panel[s]] = s;
+    for (int32_t s = 0; s < ntgt; ++s) dslot[pl->tgt_slot_panel[s]] = s;
+    if (tree) {
+        for (int k = 0; k < np; ++k) {
+            const Panel &q = t.p[k];
+            if (q.count() == 0 || q.parent < 1) continue;
+            const int par = q.parent - 1;
+            if (wslot[k] < 0 && wslot[par] >= 0) { wslot[k] = nw++; wpanel.push_back(k); }
+            if (dslot[k] < 0 && dslot[par] >= 0) { dslot[k] = ndn++; dpanel.push_back(k); }
+        }
+    }
+    pl->n_wslots = nw;
+    pl->n_dslots = ndn;
+    auto nodes_of = [&](const std::vector<int32_t> &panels, std::vector<double> &out) {
+        out.assign(panels.size() * 2 * (size_t)nd, 0.0);
+        for (size_t i = 0; i < panels.size(); ++i) {
+            const Panel &q = t.p[panels[i]];
+            cheb_nodes(q.min_xi, q.max_xi, d, &out[i * 2 * nd]);
+            cheb_nodes(q.min_eta, q.max_eta, d, &out[i * 2 * nd + nd]);
+        }
+    };
+    nodes_of(wpanel, pl->tc_up_nodes);
+    nodes_of(dpanel, pl->tc_down_nodes);
+    pl->m2m_tasks.clear();
+    pl->m2m_level_beg.clear();
+    pl->l2l_tasks.clear();
+    pl->l2l_level_beg.clear();
+    if (tree) {
+        const int maxl = t.max_level();
+        std::vector<std::vector<int32_t>> up(maxl + 1), down(maxl + 1);
+        for (int k = 0; k < np; ++k) {
+            const Panel &q = t.p[k];
+            if (wslot[k] >= 0 && !q.is_leaf && q.count() > 0) up[q.level].push_back(k);
+            if (dslot[k] >= 0 && q.parent >= 1 && dslot[q.parent - 1] >= 0) down[q.level].push_back(k);
+        }
+        for (int l = maxl; l >= 0; --l) {
+            if (up[l].empty()) continue;
+            pl->m2m_level_beg.push_back((int32_t)(pl->m2m_tasks.size() / 5));
+            for (int k : up[l]) {
+                pl->m2m_tasks.push_back(wslot[k]);
+                for (int c = 0; c < 4; ++c) {
+                    const int ch = t.p[k].child[c];
+                    pl->m2m_tasks.push_back(ch >= 1 && t.p[ch - 1].count() > 0 ? wslot[ch - 1] : -1);
+                }
+            }
+        }
+        pl->m2m_level_beg.push_back((int32_t)(pl->m2m_tasks.size() / 5));
+        for (int l = 0; l <= maxl; ++l) {
+            if (down[l].empty()) continue;
+            pl->l2l_level_beg.push_back((int32_t)(pl->l2l_tasks.size() / 3));
+            for (int k : down[l]) {
+                pl->l2l_tasks.push_back(dslot[k]);
+                pl->l2l_tasks.push_back(dslot[t.p[k].parent - 1]);
+                pl->l2l_tasks.push_back(tgt_slot[k] >= 0 ? 1 : 0);
+            }
+        }
+        pl->l2l_level_beg.push_back((int32_t)(pl->l2l_tasks.size() / 3));
+    }
+
+    // ---- the split weight store's row map
     pl->tc_items.clear();
     pl->tc_proxy_items.clear();
     pl->tc_proxy_groups.clear();
@@ -360,125 +475,208 @@ bool plan_build(const Tree &t, int d, int mode, const int32_t *list, int64_t nli
     pl->bsrc.clear();
     pl->sloc_ranges.clear();
     pl->sloc_centres.clear();
-    if (dtt) {
-        auto add_range = [&](int64_t b, int64_t e, int k) {
-            pl->sloc_ranges.push_back((int32_t)b);
-            pl->sloc_ranges.push_back((int32_t)e);
-            pl->sloc_centres.push_back(t.cx[k]);
-            pl->sloc_centres.push_back(t.cy[k]);
-            pl->sloc_centres.push_back(t.cz[k]);
-        };
-        for (int k : leaves) add_range(t.p[k].begin, t.p[k].end, k);
-        for (int32_t s = 0; s < nsrc; ++s) add_range(n + (int64_t)s * P, n + (int64_t)(s + 1) * P, pl->src_slot_panel[s]);
-        auto up8 = [](int64_t x) { return (x + 7) & ~int64_t(7); };
-        std::vector<int64_t> leaf_b(leaves.size());
-        int64_t nb = 0;
-        for (size_t i = 0; i < leaves.size(); ++i) { leaf_b[i] = nb; nb += up8(t.p[leaves[i]].count()); }
-        const int64_t src_b0 = nb, P8 = up8(P), P38 = up8(3 * P);
-        pl->tc_pt_ksteps = src_b0 / 8;
-        nb += (int64_t)nsrc * P8;
-        const int64_t phi_b0 = nb;
-        pl->tc_src_ksteps = phi_b0 / 8;
-        nb += (int64_t)ntgt * P38;
-        if (nb / 8 > INT32_MAX / 2) { *err = "grid too large for the split weight store"; return false; }
-        pl->bsrc.assign((size_t)nb, -1);
-        for (size_t i = 0; i < leaves.size(); ++i) {
-            const Panel &q = t.p[leaves[i]];
-            for (int64_t p = q.begin; p < q.end; ++p) pl->bsrc[leaf_b[i] + (p - q.begin)] = (int32_t)p;
-        }
-        for (int32_t s = 0; s < nsrc; ++s)
-            for (int r = 0; r < P; ++r) pl->bsrc[src_b0 + s * P8 + r] = (int32_t)(n + (int64_t)s * P + r);
-        for (int32_t s = 0; s < ntgt; ++s)
-            for (int r = 0; r < 3 * P; ++r) pl->bsrc[phi_b0 + s * P38 + r] = (int32_t)(-2 - ((int64_t)s * 3 * P + r));
-        // One work list (items [ib, ie) of `src`) as tcgen05 items relative to
-        // the centre of target panel kt, with the accumulator-chain flags.
-        auto convert = [&](const std::vector<Item> &src, int32_t ib0, int32_t ie0, int kt,
-                           std::vector<TcItem> &dst) -> bool {
-            const int32_t ib = (int32_t)dst.size();
-            auto push = [&](int kind, int64_t off, int64_t total, int64_t base, int ks) {
-                TcItem r{};
-                r.kind = kind;
-                if (ks >= 0) {
-                    r.dx = (float)(t.cx[ks] - t.cx[kt]);
-                    r.dy = (float)(t.cy[ks] - t.cy[kt]);
-                    r.dz = (float)(t.cz[ks] - t.cz[kt]);
-                }
-                for (int64_t b = 0; b < total; b += kTcChunk) {
-                    r.cnt = (int32_t)std::min<int64_t>(kTcChunk, total - b);
-                    r.kb = (int32_t)((base + b) / 8);
-                    r.off = (int32_t)(kind == 2 ? off : off + b);
-                    r.row0 = kind == 2 ? (int32_t)b : 0;
-                    dst.push_back(r);
-                }
-            };
-            for (int32_t i = ib0; i < ie0; ++i) {
-                const Item &it = src[i];
-                if (it.kind == 0) {
-                    // a point source panel's range, re-joined across the
-                    // staging splits and cut at leaf boundaries
-                    int64_t b = it.off, e = (int64_t)it.off + it.cnt;
-                    while (i + 1 < ie0 && src[i + 1].kind == 0 && src[i + 1].off == e) e += src[++i].cnt;
-                    while (b < e) {
-                        const int32_t l = leaf_of_pos[b];
-                        const Panel &q = t.p[leaves[l]];
-                        const int64_t le = std::min<int64_t>(e, q.end);
-                        if ((b - q.begin) % 8 != 0) { *err = "internal: point range starts inside a leaf"; return false; }
-                        push(0, b, le - b, leaf_b[l] + (b - q.begin), leaves[l]);
-                        b = le;
-                    }
-                } else if (it.kind == 1) {
-                    const int64_t s = ((int64_t)it.off - n) / P;
-                    push(1, it.off, it.cnt, src_b0 + s * P8, pl->src_slot_panel[s]);
-                } else {
-                    push(2, it.off, 3 * P, phi_b0 + (int64_t)it.off * P38, -1);
-                }
+    pl->tc_leaf_groups.clear();
+    auto add_range = [&](int64_t b, int64_t e, int k) {
+        pl->sloc_ranges.push_back((int32_t)b);
+        pl->sloc_ranges.push_back((int32_t)e);
+        pl->sloc_centres.push_back(t.cx[k]);
+        pl->sloc_centres.push_back(t.cy[k]);
+        pl->sloc_centres.push_back(t.cz[k]);
+    };
+    for (int k : leaves) add_range(t.p[k].begin, t.p[k].end, k);
+    for (int32_t s = 0; s < nsrc; ++s) add_range(n + (int64_t)s * P, n + (int64_t)(s + 1) * P, pl->src_slot_panel[s]);
+    auto up8 = [](int64_t x) { return (x + 7) & ~int64_t(7); };
+    std::vector<int64_t> leaf_b(leaves.size());
+    int64_t nb = 0;
+    for (size_t i = 0; i < leaves.size(); ++i) { leaf_b[i] = nb; nb += up8(t.p[leaves[i]].count()); }
+    const int64_t src_b0 = nb, P8 = up8(P), P38 = up8(3 * P);
+    pl->tc_pt_ksteps = src_b0 / 8;
+    nb += (int64_t)nsrc * P8;
+    const int64_t phi_b0 = nb;
+    pl->tc_src_ksteps = phi_b0 / 8;
+    // potential blocks: per target slot (direct) or per leaf below a target
+    // slot (tree); phi_blocks[b] = the dslot whose rows block b holds
+    std::vector<int32_t> phi_blocks, leaf_phi_block(leaves.size(), -1);
+    if (tree) {
+        for (size_t i = 0; i < leaves.size(); ++i)
+            if (dslot[leaves[i]] >= 0) { leaf_phi_block[i] = (int32_t)phi_blocks.size(); phi_blocks.push_back(dslot[leaves[i]]); }
+    } else {
+        for (int32_t s = 0; s < ntgt; ++s) phi_blocks.push_back(s);
+    }
+    nb += (int64_t)phi_blocks.size() * P38;
+    if (nb / 8 > INT32_MAX / 2) { *err = "grid too large for the split weight store"; return false; }
+    pl->bsrc.assign((size_t)nb, -1);
+    for (size_t i = 0; i < leaves.size(); ++i) {
+        const Panel &q = t.p[leaves[i]];
+        for (int64_t r = q.begin; r < q.end; ++r) pl->bsrc[leaf_b[i] + (r - q.begin)] = (int32_t)r;
+    }
+    for (int32_t s = 0; s < nsrc; ++s)
+        for (int r = 0; r < P; ++r) pl->bsrc[src_b0 + s * P8 + r] = (int32_t)(n + (int64_t)s * P + r);
+    for (size_t b = 0; b < phi_blocks.size(); ++b)
+        for (int r = 0; r < 3 * P; ++r)
+            pl->bsrc[phi_b0 + (int64_t)b * P38 + r] = (int32_t)(-2 - ((int64_t)phi_blocks[b] * 3 * P + r));
+
+    // One work list (items [ib, ie) of `src`) as tcgen05 items relative to the
+    // centre of target panel kt, with the accumulator-chain flags.  DOWN items
+    // of the direct passes read their target slot's potential block.
+    auto convert = [&](const std::vector<Item> &src, int32_t ib0, int32_t ie0, int kt, std::vector<TcItem> &dst,
+                       int32_t extra_down_leaf) -> bool {
+        const int32_t ib = (int32_t)dst.size();
+        auto push = [&](int kind, int64_t off, int64_t total, int64_t base, int ks) {
+            TcItem r{};
+            r.kind = kind;
+            if (ks >= 0) {
+                r.dx = (float)(t.cx[ks] - t.cx[kt]);
+                r.dy = (float)(t.cy[ks] - t.cy[kt]);
+                r.dz = (float)(t.cz[ks] - t.cz[kt]);
             }
-            const int32_t ie = (int32_t)dst.size();
-            // accumulator chains: end one after the item that brings it to
-            // kTcChainKSteps k-steps, and always after the list's last item
-            for (int32_t i = ib, chain = 0; i < ie; ++i) {
-                TcItem &r = dst[i];
-                chain += (r.cnt + 7) / 8;
-                if (chain >= kTcChainKSteps || i == ie - 1) { r.kind |= kTcFlush; chain = 0; }
+            for (int64_t b = 0; b < total; b += kTcChunk) {
+                r.cnt = (int32_t)std::min<int64_t>(kTcChunk, total - b);
+                r.kb = (int32_t)((base + b) / 8);
+                r.off = (int32_t)(kind == 2 ? off : off + b);
+                r.row0 = kind == 2 ? (int32_t)b : 0;
+                dst.push_back(r);
             }
-            return true;
         };
-        std::vector<int32_t> gord(pl->leaf_groups.size());
-        std::iota(gord.begin(), gord.end(), 0);
-        std::sort(gord.begin(), gord.end(), [&](int a, int b) { return pl->leaf_groups[a].tgt < pl->leaf_groups[b].tgt; });
-        for (int32_t gi : gord) {
-            const Group &g = pl->leaf_groups[gi];
-            const int kt = leaves[g.out];
-            const int32_t ib = (int32_t)pl->tc_items.size();
-            if (!convert(pl->leaf_items, g.ib, g.ie, kt, pl->tc_items)) return false;
-            const int32_t ie = (int32_t)pl->tc_items.size();
-            for (int32_t r = 0; r < g.nt; r += kTcRows) {
-                MixGroup m{};
-                m.tgt = g.tgt + r; m.nt = std::min(kTcRows, g.nt - r); m.ib = ib; m.ie = ie; m.out = g.out;
-                m.cx = t.cx[kt]; m.cy = t.cy[kt]; m.cz = t.cz[kt];
-                pl->tc_leaf_groups.push_back(m);
+        for (int32_t i = ib0; i < ie0; ++i) {
+            const Item &it = src[i];
+            if (it.kind == 0) {
+                // a point source panel's range, re-joined across the
+                // staging splits and cut at leaf boundaries
+                int64_t b = it.off, e = (int64_t)it.off + it.cnt;
+                while (i + 1 < ie0 && src[i + 1].kind == 0 && src[i + 1].off == e) e += src[++i].cnt;
+                while (b < e) {
+                    const int32_t l = leaf_of_pos[b];
+                    const Panel &q = t.p[leaves[l]];
+                    const int64_t le = std::min<int64_t>(e, q.end);
+                    if ((b - q.begin) % 8 != 0) { *err = "internal: point range starts inside a leaf"; return false; }
+                    push(0, b, le - b, leaf_b[l] + (b - q.begin), leaves[l]);
+                    b = le;
+                }
+            } else if (it.kind == 1) {
+                const int64_t s = ((int64_t)it.off - n) / P;
+                push(1, it.off, it.cnt, src_b0 + s * P8, pl->src_slot_panel[s]);
+            } else if (!tree) {
+                push(2, it.off, 3 * P, phi_b0 + (int64_t)it.off * P38, -1);
             }
         }
-        // proxy pass: per unit of a target slot, rows of at most kTcProxyRows
-        // proxies (three Cartesian components each fill the MMA's N = 256)
-        for (const Group &g : pl->proxy_groups) {
-            const int kt = pl->tgt_slot_panel[g.tgt];
+        if (extra_down_leaf >= 0 && leaf_phi_block[extra_down_leaf] >= 0)
+            push(2, dslot[leaves[extra_down_leaf]], 3 * P, phi_b0 + (int64_t)leaf_phi_block[extra_down_leaf] * P38, -1);
+        const int32_t ie = (int32_t)dst.size();
+        // accumulator chains: end one after the item that brings it to
+        // chain_ksteps k-steps, and always after the list's last item
+        for (int32_t i = ib, chain = 0; i < ie; ++i) {
+            TcItem &r = dst[i];
+            chain += (r.cnt + 7) / 8;
+            if (chain >= opt.chain_ksteps || i == ie - 1) { r.kind |= kTcFlush; chain = 0; }
+        }
+        return true;
+    };
+
+    // ---- leaf pass: groups of at most kTcRows targets in pool order
+    std::vector<int32_t> gord(pl->leaf_groups.size());
+    std::iota(gord.begin(), gord.end(), 0);
+    std::sort(gord.begin(), gord.end(), [&](int a, int b) { return pl->leaf_groups[a].tgt < pl->leaf_groups[b].tgt; });
+    pl->tc_macs_down = 0;
+    for (int32_t gi : gord) {
+        const Group &g = pl->leaf_groups[gi];
+        const int kt = leaves[g.out];
+        const int32_t ib = (int32_t)pl->tc_items.size();
+        if (!convert(pl->leaf_items, g.ib, g.ie, kt, pl->tc_items, tree ? g.out : -1)) return false;
+        const int32_t ie = (int32_t)pl->tc_items.size();
+        if (tree && leaf_phi_block[g.out] >= 0) pl->tc_macs_down += (double)g.nt * P;
+        for (int32_t r = 0; r < g.nt; r += kTcRows) {
+            MixGroup m{};
+            m.tgt = g.tgt + r; m.nt = std::min(kTcRows, g.nt - r); m.ib = ib; m.ie = ie; m.out = g.out;
+            m.cx = t.cx[kt]; m.cy = t.cy[kt]; m.cz = t.cz[kt];
+            pl->tc_leaf_groups.push_back(m);
+        }
+    }
+    if (!tree) pl->tc_macs_down = pl->macs_down;
+
+    // ---- proxy pass: each target slot's items cut into units of at most
+    // proxy_unit_kpairs * 1024 pairs; rows of at most kTcProxyRows proxies
+    // (three Cartesian components each fill the MMA's N = 256)
+    {
+        const double budget = 1024.0 * opt.proxy_unit_kpairs;
+        pl->tc_proxy_unit_beg.assign(ntgt + 1, 0);
+        struct U { int32_t slot, ib, ie; double cost; };
+        std::vector<U> units;
+        for (int32_t s = 0; s < ntgt; ++s) {
+            pl->tc_proxy_unit_beg[s] = (int32_t)units.size();
+            int32_t i = pl->proxy_slot_items[s];
+            const int32_t e = pl->proxy_slot_items[s + 1];
+            while (i < e) {
+                U u{s, i, i, 0.0};
+                while (u.ie < e && (u.cost == 0 || u.cost + (double)pl->proxy_items[u.ie].cnt * P <= budget)) {
+                    u.cost += (double)pl->proxy_items[u.ie].cnt * P;
+                    ++u.ie;
+                }
+                i = u.ie;
+                units.push_back(u);
+            }
+        }
+        pl->tc_proxy_unit_beg[ntgt] = (int32_t)units.size();
+        pl->tc_nproxy_units = (int32_t)units.size();
+        std::vector<int32_t> ord(units.size());
+        std::iota(ord.begin(), ord.end(), 0);
+        std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) { return units[a].cost > units[b].cost; });
+        for (int32_t uo : ord) {
+            const U &u = units[uo];
+            const int kt = pl->tgt_slot_panel[u.slot];
             const int32_t ib = (int32_t)pl->tc_proxy_items.size();
-            if (!convert(pl->proxy_items, g.ib, g.ie, kt, pl->tc_proxy_items)) return false;
+            if (!convert(pl->proxy_items, u.ib, u.ie, kt, pl->tc_proxy_items, -1)) return false;
             const int32_t ie = (int32_t)pl->tc_proxy_items.size();
             for (int32_t r = 0; r < P; r += kTcProxyRows) {
                 MixGroup m{};
-                m.tgt = g.tgt; m.nt = std::min(kTcProxyRows, P - r); m.ib = ib; m.ie = ie; m.out = g.out; m.row0 = r;
+                m.tgt = u.slot; m.nt = std::min(kTcProxyRows, P - r); m.ib = ib; m.ie = ie; m.out = uo; m.row0 = r;
                 m.cx = t.cx[kt]; m.cy = t.cy[kt]; m.cz = t.cz[kt];
                 pl->tc_proxy_groups.push_back(m);
             }
         }
-        // upward pass: per source slot, units of whole leaves of its panel
-        // (at least kUpChunk points, or the panel's rest), rows of at most
-        // kTcRows proxies; every item gets its own k-steps in the basis store
-        pl->tc_up_unit_beg.assign(nsrc + 1, 0);
-        int32_t nunits = 0;
-        int64_t nbk = 0;
+    }
+
+    // ---- upward pass.  Direct: per source slot, units of whole leaves of
+    // its panel (at least up_chunk points, or the panel's rest).  Tree: one
+    // unit per leaf below a source slot, written straight to the leaf's
+    // wslot rows.  Rows of at most kTcRows proxies; every item gets its own
+    // k-steps in the basis store (per-point BLI factors over the nodes of
+    // the unit's panel: tc_bas holds nodes slot, first pool row, rows).
+    pl->tc_up_unit_beg.assign(nsrc + 1, 0);
+    int32_t nunits = 0;
+    int64_t nbk = 0;
+    pl->tc_macs_up = 0;
+    auto add_unit = [&](int ks, int64_t b, int64_t e, int32_t out, int32_t nodes_slot) -> bool {
+        const std::vector<Item> range{Item{(int32_t)b, (int32_t)(e - b), -1, 0}};
+        const int32_t ib = (int32_t)pl->tc_up_items.size();
+        if (!convert(range, 0, 1, ks, pl->tc_up_items, -1)) return false;
+        const int32_t ie = (int32_t)pl->tc_up_items.size();
+        for (int32_t i = ib; i < ie; ++i) {
+            TcItem &r = pl->tc_up_items[i];
+            r.row0 = (int32_t)nbk;
+            for (int32_t k = 0; k < r.cnt; k += 8) {
+                pl->tc_bas.push_back(nodes_slot);
+                pl->tc_bas.push_back(r.off + k);
+                pl->tc_bas.push_back(std::min(8, r.cnt - k));
+                ++nbk;
+            }
+        }
+        for (int32_t r = 0; r < P; r += kTcRows) {
+            MixGroup m{};
+            m.tgt = nodes_slot; m.nt = std::min(kTcRows, P - r); m.ib = ib; m.ie = ie; m.out = out; m.row0 = r;
+            pl->tc_up_groups.push_back(m);
+        }
+        pl->tc_macs_up += (double)(e - b) * P;
+        return true;
+    };
+    if (tree) {
+        for (size_t i = 0; i < leaves.size(); ++i) {
+            const int k = leaves[i];
+            if (wslot[k] < 0) continue;
+            if (!add_unit(k, t.p[k].begin, t.p[k].end, wslot[k], wslot[k])) return false;
+            ++nunits;
+        }
+    } else {
         for (int32_t s = 0; s < nsrc; ++s) {
             const int ks = pl->src_slot_panel[s];
             pl->tc_up_unit_beg[s] = nunits;
@@ -488,36 +686,15 @@ bool plan_build(const Tree &t, int d, int mode, const int32_t *list, int64_t nli
                 const int64_t b = t.p[leaves[l]].begin;
                 int64_t e = b;
                 int32_t l2 = l;
-                while (l2 < le && e - b < kUpChunk) e = t.p[leaves[l2++]].end;
-                const std::vector<Item> range{Item{(int32_t)b, (int32_t)(e - b), -1, 0}};
-                const int32_t ib = (int32_t)pl->tc_up_items.size();
-                if (!convert(range, 0, 1, ks, pl->tc_up_items)) return false;
-                const int32_t ie = (int32_t)pl->tc_up_items.size();
-                for (int32_t i = ib; i < ie; ++i) {
-                    TcItem &r = pl->tc_up_items[i];
-                    r.row0 = (int32_t)nbk;
-                    for (int32_t k = 0; k < r.cnt; k += 8) {
-                        pl->tc_bas.push_back(s);
-                        pl->tc_bas.push_back(r.off + k);
-                        pl->tc_bas.push_back(std::min(8, r.cnt - k));
-                        ++nbk;
-                    }
-                }
-                for (int32_t r = 0; r < P; r += kTcRows) {
-                    MixGroup m{};
-                    m.tgt = s; m.nt = std::min(kTcRows, P - r); m.ib = ib; m.ie = ie; m.out = nunits; m.row0 = r;
-                    pl->tc_up_groups.push_back(m);
-                }
+                while (l2 < le && e - b < opt.up_chunk) e = t.p[leaves[l2++]].end;
+                if (!add_unit(ks, b, e, nunits, s)) return false;
                 ++nunits;
                 l = l2;
             }
         }
         pl->tc_up_unit_beg[nsrc] = nunits;
-        if (nbk > INT32_MAX / 2) { *err = "grid too large for the basis store"; return false; }
     }
-    // ---------------------------------------------------------------- point data in pool order
-    pl->pxi.resize(n); pl->peta.resize(n);
-    for (int32_t p = 0; p < n; ++p) { pl->pxi[p] = t.xi[t.order[p]]; pl->peta[p] = t.eta[t.order[p]]; }
+    if (nbk > INT32_MAX / 2) { *err = "grid too large for the basis store"; return false; }
     return true;
 }
 

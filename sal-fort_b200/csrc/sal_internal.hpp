@@ -97,6 +97,18 @@ struct TcItem {
     int32_t row0;
 };
 
+// Runtime choices of the batched form's tcgen05 passes: the search space of
+// the autotuner (sal_grid_autotune).  Changing them re-cuts the tcgen05 part
+// of the plan; the FP64 plan is unaffected.
+struct TcOptions {
+    int32_t chain_ksteps = 32;          // k-steps an accumulator chain reaches before it is folded
+    int32_t tree_passes = 1;            // 1: leaf-level upward + child-to-parent transfers, parent-to-child
+                                        //    transfers + one DOWN item per leaf; 0: direct per-slot passes
+    int32_t up_chunk = 4096;            // direct upward pass: points per work unit at least
+    int32_t proxy_unit_kpairs = 648;    // proxy pass: kernel pairs of a work unit, in units of 1024
+    int32_t cta_groups = 1;             // tcgen05 launches: groups a CTA walks at most
+};
+
 struct Plan {
     int32_t n = 0, d = 0, P = 0, mode = 0, npanels = 0, nleaves = 0;
     // point data in pool order (leaf-contiguous DFS)
@@ -149,6 +161,23 @@ struct Plan {
     std::vector<int32_t> sloc_ranges;
     std::vector<double> sloc_centres;
     std::vector<Item> mix_leaf_items, mix_proxy_items;
+    std::vector<int32_t> proxy_slot_items;        // tgt slot -> first item in proxy_items (ntgt + 1)
+    // tcgen05 proxy pass units: the plan's own cut of each target slot's
+    // items (tc_proxy_unit_beg: tgt slot -> first unit, ntgt + 1)
+    std::vector<int32_t> tc_proxy_unit_beg;
+    int32_t tc_nproxy_units = 0;
+    // tree passes of the batched form.  Proxy-weight slots ("wslots"): the
+    // source slots, then every other panel with points below a source slot;
+    // potential slots ("dslots"): the target slots, then every other panel
+    // with points below a target slot.  Nodes per slot: 2(d+1) (xi, then eta).
+    TcOptions tc_opt;
+    int32_t n_wslots = 0, n_dslots = 0;
+    std::vector<double> tc_up_nodes, tc_down_nodes;
+    std::vector<int32_t> m2m_tasks;               // per refined up panel: parent wslot, 4 child wslots (-1: none)
+    std::vector<int32_t> m2m_level_beg;           // task ranges per level, deepest first
+    std::vector<int32_t> l2l_tasks;               // per down panel under another: child dslot, parent dslot, own
+    std::vector<int32_t> l2l_level_beg;           // task ranges per level, top first
+    double tc_macs_up = 0, tc_macs_down = 0;      // per field: basis MACs of the batched form's upward / DOWN work
     double pairs[4] = {0, 0, 0, 0};               // PP, PC, CP, CC evaluations per field
     double macs_up = 0, macs_down = 0;
     int32_t max_nt = 0;
@@ -157,6 +186,8 @@ struct Plan {
 // Builds the plan of a DTT list (triplets) or STT lists (pairs).
 bool plan_build(const Tree &t, int d, int mode, const int32_t *list, int64_t nlist, const int32_t *pc, int64_t npc,
                 const int32_t *pp, int64_t npp, Plan *plan, std::string *err);
+// (Re)builds the tcgen05 part of a DTT plan for the given options.
+bool plan_build_tc(const Tree &t, Plan *plan, const TcOptions &opt, std::string *err);
 
 constexpr int kMaxStage = 256;   // sources staged per item (items are split to fit)
 constexpr int kMixStage = 64;    // sources (or DOWN rows) staged per batched item
@@ -164,7 +195,8 @@ constexpr int kMixRows = 64;     // targets per batched CTA
 constexpr int kTcRows = 128;     // targets per tcgen05 leaf group (the MMA's M)
 constexpr int kTcChunk = 64;     // sources (or DOWN rows) per tcgen05 item
 constexpr int kTcProxyRows = 85;   // target proxies per tcgen05 proxy group: 3 x 85 <= 256
-constexpr int kTcChainKSteps = 32;  // k-steps (8 sources) an accumulator chain reaches before it is folded
 constexpr int kMaxDegree = 14;   // a DOWN record (4(d+1)^2 + 2(d+1) doubles) fits one 8 KB stage
+constexpr int kMaxTreeDegree = 10;  // tree transfers of the batched form: their tiles fit shared memory up to here
+constexpr int kMaxTreeP = (kMaxTreeDegree + 1) * (kMaxTreeDegree + 1);
 
 }  // namespace sal

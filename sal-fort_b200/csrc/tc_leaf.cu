@@ -26,15 +26,12 @@
 //               branch).  The self pair enters as the tile's diagonal entry:
 //               the reference kernel's FP64 value at distance zero (rounding
 //               noise).  The sources' FP32 coordinates (per k-step x[8] y[8]
-//               z[8]) are read from global memory into registers a task
-//               ahead.  A stage costs the latency of the busiest warp's tasks
-//               (dependent arithmetic and shared-memory round trips), not
-//               their issue: more warps on fewer tasks each is what helps.
+//               z[8]) come from shared memory, copied there by the loader.
 //   warp 8      issues the MMAs.
 //   warp 9      loads, per stage, the weight tiles (pre-split TF32 hi / lo,
-//               written once per solve by split_store_kernel), and for the
-//               upward pass the BLI factors, with bulk copies into a 3-deep
-//               ring.
+//               written once per solve by split_store_kernel) and the
+//               sources' coordinates (leaf and proxy passes) or BLI factors
+//               (upward pass), with bulk copies into a 3-deep ring.
 //   warps 10-13 fold finished accumulator chains into the running sums and
 //               write the outputs (warp w: tensor memory lanes 32(w%4)..+31).
 // The tensor cores accumulate with truncation, so one chain over all of a
@@ -68,7 +65,6 @@ constexpr int kStageK = 32;                       // K columns per stage (four k
 constexpr int kStageKs = kStageK / 8;             // k-steps per stage
 constexpr int kKStages = 2;                       // kernel-tile ring
 constexpr int kWStages = 3;                       // weight / upward-factor ring
-constexpr int kMaxGroupsPerCta = 1;               // CTAs stay short (see launch_tc)
 constexpr int kAuxFloats = kStageKs * 16 * (kMaxDegree + 1);   // upward factors of a stage's k-steps
 constexpr int kTileFloats = 2048;                 // kernel tile of one k-step: 256 rows x 8, one of hi / lo
 constexpr int kWStepFloats = 1024;                // weight tile of one k-step: 128 rows x 8
@@ -358,27 +354,10 @@ __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(TcArgs a, int *err
         //   3-4 row blocks: warp w takes row block w % 4, k-steps w / 4, w / 4 + 2
         //   2 row blocks:   warp w takes row block w % 2, k-step w / 2
         //   1 row block:    warp w < 4 takes k-step w (warps 4-7 only arrive)
-        // Source coordinates of k-step kk of stage jj of item x (x[8] y[8]
-        // z[8] in the per-k-step store), or null where the item has no such
-        // k-step or no point sources.  The leaf and proxy passes read them
-        // from global memory into registers one task ahead, so no
-        // shared-memory round trip sits between the slot check and the
-        // arithmetic.
-        auto kptr = [&](const TcItem &x, int jj, int kk) -> const float4 * {
-            const int ki = kStageKs * jj + kk;
-            return (MODE != 2 && (x.kind & 3) != 2 && 8 * ki < x.cnt)
-                       ? reinterpret_cast<const float4 *>(a.sxyz + (size_t)(x.kb + ki) * 24)
-                       : nullptr;
-        };
-        float4 pre[6] = {};
-        const float4 *pre_src = nullptr;   // where pre was loaded from
-        auto fetch = [&](const float4 *p) {
-            if (p) {
-#pragma unroll
-                for (int i = 0; i < 6; ++i) pre[i] = __ldg(p + i);
-            }
-            pre_src = p;
-        };
+        // The source coordinates of a stage's k-steps (x[8] y[8] z[8] each,
+        // relative to their panel's centre) arrive in shared memory with the
+        // stage's weights: the loader warp copies them up to kWStages stages
+        // ahead, so no global-memory latency sits in a producer task.
 
         for (int gi = blockIdx.x; gi < a.ngroups; gi += gridDim.x) {
             const MixGroup G = a.groups[gi];
@@ -442,7 +421,6 @@ __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(TcArgs a, int *err
             // item records are read one item ahead, so their latency hides
             // behind the current item's stages
             TcItem nxt = a.items[G.ib];
-            if (active) fetch(kptr(nxt, 0, kfirst));
             for (int k = 0; k < ni; ++k) {
                 const TcItem it = nxt;
                 if (k + 1 < ni) nxt = a.items[G.ib + k + 1];
@@ -473,14 +451,13 @@ __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(TcArgs a, int *err
                     // the MMAs that last read this slot must be done before
                     // the first store into it
                     bool slot_free = st < (uint32_t)kKStages;
-                    if (MODE == 2 && active && kfirst < nks)
+                    // the stage's upward factors (MODE 2) or source
+                    // coordinates (point and proxy sources) are in aux
+                    if ((MODE == 2 || kind != 2) && active && kfirst < nks)
                         wait_bounded(&sm.wfull[st % kWStages], (st / kWStages) & 1, abort, err);
+                    const float4 *crd = reinterpret_cast<const float4 *>(sm.aux[st % kWStages]);
 #pragma unroll 1
                     for (int kk = kfirst; active && kk < nks; kk += kstride) {
-                        if (MODE != 2 && kind != 2) {
-                            const float4 *want = kptr(it, j, kk);
-                            if (want != pre_src) fetch(want);   // not prefetched: load now
-                        }
                         float ve[8], vn[8], vz[8];
                         if (MODE == 2) {
                             // upward: the BLI basis of proxy (i, j) at the 8 points,
@@ -510,6 +487,11 @@ __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(TcArgs a, int *err
                         } else {
                             // PP / PC: kernel value x projected displacement,
                             // two columns per packed instruction
+                            // this k-step's x[8] y[8] z[8] (same address in every
+                            // lane: shared-memory broadcasts)
+                            float4 pre[6];
+#pragma unroll
+                            for (int i = 0; i < 6; ++i) pre[i] = crd[6 * kk + i];
 #pragma unroll
                             for (int c2 = 0; c2 < 4; ++c2) {
                                 // pre[0..1] = x[8], pre[2..3] = y[8], pre[4..5] = z[8]
@@ -556,14 +538,6 @@ __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(TcArgs a, int *err
                                 }
                             }
                         }
-                        // the next task's coordinates: its next k-step in this
-                        // stage, else its first of the next stage or item
-                        // (issued once this task's are consumed)
-                        if (MODE != 2)
-                            fetch(kk + kstride < nks ? kptr(it, j, kk + kstride)
-                                  : j + 1 < nst      ? kptr(it, j + 1, kfirst)
-                                  : k + 1 < ni       ? kptr(nxt, 0, kfirst)
-                                                     : nullptr);
                         if (!slot_free) {
                             wait_bounded(&sm.kempty[slot], kpar, abort, err);
                             slot_free = true;
@@ -676,15 +650,18 @@ __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(TcArgs a, int *err
                     if (lane == 0) {
                         const int ncol = min(kStageK, it.cnt - kStageK * j), nks = (ncol + 7) >> 3;
                         const uint32_t wbytes = (uint32_t)nks * kWStepFloats * 4;
-                        // upward: the stage's BLI factors come with the weights
-                        // (the other passes' producers read source coordinates
-                        // themselves)
-                        const uint32_t lbytes = MODE == 2 ? (uint32_t)nks * 64 * n : 0u;
+                        // with the weights: the stage's BLI factors (upward) or
+                        // its point / proxy sources' coordinates (24 floats per
+                        // k-step; DOWN rows need none)
+                        const uint32_t lbytes = MODE == 2 ? (uint32_t)nks * 64 * n
+                                                : (it.kind & 3) != 2 ? (uint32_t)nks * 96u : 0u;
                         dev::mbar_expect_tx(&sm.wfull[jb], wbytes + lbytes);
                         if (!*abort) {
                             if (lbytes)
-                                dev::bulk_g2s(sm.aux[jb], a.basis + (size_t)(it.row0 + kStageKs * j) * 16 * n, lbytes,
-                                              &sm.wfull[jb]);
+                                dev::bulk_g2s(sm.aux[jb],
+                                              MODE == 2 ? (const void *)(a.basis + (size_t)(it.row0 + kStageKs * j) * 16 * n)
+                                                        : (const void *)(a.sxyz + (size_t)(it.kb + kStageKs * j) * 24),
+                                              lbytes, &sm.wfull[jb]);
                             dev::bulk_g2s(sm.Wt[jb], a.bstore + (size_t)(it.kb + kStageKs * j) * kWStepFloats, wbytes,
                                           &sm.wfull[jb]);
                         }
@@ -835,21 +812,23 @@ size_t tc_smem_bytes() {
 }
 
 template <int MODE>
-static void launch_tc(const TcArgs &a, int nsm, int *err, cudaStream_t st) {
+static void launch_tc(const TcArgs &a, int nsm, int cta_groups, int *err, cudaStream_t st) {
     if (a.ngroups <= 0) return;
     const size_t smem = tc_smem_bytes();
     static std::atomic<unsigned long long> done{0};
     smem_attr_once((const void *)tc_leaf_kernel<MODE>, (int)smem, done);
-    // every SM busy, but no CTA longer than kMaxGroupsPerCta groups, so that
-    // kernels of other streams (higher-priority grids) get SMs as CTAs retire
-    int grid = (a.ngroups + kMaxGroupsPerCta - 1) / kMaxGroupsPerCta;
+    // every SM busy, but no CTA longer than cta_groups groups: with short
+    // CTAs, kernels of other streams (higher-priority grids) get SMs as CTAs
+    // retire
+    const int per = cta_groups > 0 ? cta_groups : 1;
+    int grid = (a.ngroups + per - 1) / per;
     if (grid < nsm) grid = a.ngroups < nsm ? a.ngroups : nsm;
     tc_leaf_kernel<MODE><<<grid, kThreads, smem, st>>>(a, err);
 }
 
-void launch_tc_leaf(const TcArgs &a, int nsm, int *err, cudaStream_t st) { launch_tc<0>(a, nsm, err, st); }
-void launch_tc_proxy(const TcArgs &a, int nsm, int *err, cudaStream_t st) { launch_tc<1>(a, nsm, err, st); }
-void launch_tc_upward(const TcArgs &a, int nsm, int *err, cudaStream_t st) { launch_tc<2>(a, nsm, err, st); }
+void launch_tc_leaf(const TcArgs &a, int nsm, int cg, int *err, cudaStream_t st) { launch_tc<0>(a, nsm, cg, err, st); }
+void launch_tc_proxy(const TcArgs &a, int nsm, int cg, int *err, cudaStream_t st) { launch_tc<1>(a, nsm, cg, err, st); }
+void launch_tc_upward(const TcArgs &a, int nsm, int cg, int *err, cudaStream_t st) { launch_tc<2>(a, nsm, cg, err, st); }
 
 void launch_split_store(const int32_t *bsrc, int64_t k0, int64_t k1, const float *wF, const float *phiF,
                         float *bstore, cudaStream_t st) {

@@ -39,7 +39,7 @@ EXPORTS = (
     "sal_grid_timing", "sal_fma_peak", "sal_direct_sum_noalloc", "sal_solve_host", "sal_solve_host_async",
     "sal_solve_host_wait", "sal_grid_set_graphs", "sal_grid_inject_timeout", "sal_fast_sum",
     "sal_mom6_proxy_source_compute", "sal_mom6_pc_compute", "sal_mom6_pp_compute", "sal_dropin_config",
-    "sal_dropin_release",
+    "sal_dropin_release", "sal_grid_tune_get", "sal_grid_tune_set", "sal_grid_autotune",
 )
 
 
@@ -68,7 +68,19 @@ class GridStats(C.Structure):
         ("pairs_pp", C.c_double), ("pairs_pc", C.c_double), ("pairs_cp", C.c_double), ("pairs_cc", C.c_double),
         ("macs_up", C.c_double), ("macs_down", C.c_double),
         ("device_bytes", C.c_int64), ("setup_seconds", C.c_double), ("mixed_bytes", C.c_int64),
+        ("macs_up_batched", C.c_double), ("macs_down_batched", C.c_double),
     ]
+
+
+class Tune(C.Structure):
+    """sal_tune: runtime choices of the batched form's tcgen05 passes."""
+    _fields_ = [
+        ("chain_ksteps", C.c_int32), ("tree_passes", C.c_int32), ("up_chunk", C.c_int32),
+        ("proxy_unit_kpairs", C.c_int32), ("cta_groups", C.c_int32), ("field_block", C.c_int32),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
 
 
 _lib = None
@@ -124,6 +136,9 @@ def lib():
         L.sal_mom6_pp_compute.argtypes = [vp, vp, vp, i64, i32, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp,
                                           vp, vp, i32, i32]
         L.sal_dropin_config.argtypes = [i32, i32]
+        L.sal_grid_tune_get.argtypes = [vp, C.POINTER(Tune)]
+        L.sal_grid_tune_set.argtypes = [vp, C.POINTER(Tune)]
+        L.sal_grid_autotune.argtypes = [vp, vp, i32, i64, i32, d, C.POINTER(Tune), C.POINTER(d), C.POINTER(d)]
         _lib = L
         return L
 
@@ -326,6 +341,27 @@ class Grid:
         outputs overwritten.  Pinned arrays make the copies asynchronous."""
         F = ssh.shape[0] if ssh.ndim == 2 else 1
         _check(lib().sal_solve_host(self.handle, _ptr(ssh), F, self.n, _ptr(out_x), _ptr(out_y), self.n, int(form)))
+
+    def tune(self, **changes):
+        """The batched form's choices (sal_grid_tune_get) as a dict; keyword
+        arguments change them first (sal_grid_tune_set)."""
+        t = Tune()
+        _check(lib().sal_grid_tune_get(self.handle, C.byref(t)))
+        if changes:
+            for k, v in changes.items():
+                setattr(t, k, int(v))
+            _check(lib().sal_grid_tune_set(self.handle, C.byref(t)))
+        return t.as_dict()
+
+    def autotune(self, ssh, ntargets=2000, max_rel_err=5e-6):
+        """sal_grid_autotune on (F, N) float64 CUDA fields (F <= 64): sets the
+        fastest setting whose first field stays within max_rel_err of the FP64
+        direct sum; returns (setting, ms of the setting, ms of the start)."""
+        ssh2 = ssh.reshape(-1, self.n).contiguous()
+        t, mb, ms = Tune(), C.c_double(), C.c_double()
+        _check(lib().sal_grid_autotune(self.handle, C.c_void_p(ssh2.data_ptr()), ssh2.shape[0], self.n, int(ntargets),
+                                       float(max_rel_err), C.byref(t), C.byref(mb), C.byref(ms)))
+        return t.as_dict(), mb.value, ms.value
 
     def inject_timeout(self, polls):
         """Test hook (sal_grid_inject_timeout): the next FP64 solve's leaf

@@ -156,3 +156,80 @@ def test_graph_replay_matches_kernel_launches():
         st.synchronize()
         assert torch.equal(ox[:5], ref2[0]) and torch.equal(oy[:5], ref2[1])
     grid.set_graphs(False)
+
+
+@pytest.mark.parametrize("degree", [8, 10])
+def test_tree_passes_match_direct_passes(degree):
+    """The batched form's tree passes (leaf-level upward pass plus
+    child-to-parent transfers; parent-to-child transfers plus one DOWN item
+    per leaf) reproduce its direct per-slot passes: the transfers are exact in
+    exact arithmetic, so the two agree to FP32 rounding, and both stay within
+    the bars against the FP64 accurate form and the direct sum.  The basis
+    work they report falls."""
+    torch = _torch()
+    S, g, hs, grid = _grid("small_20000", 60, 4, seed=2, degree=degree)
+    ssh = torch.tensor(hs, device="cuda")
+    assert grid.tune()["tree_passes"] == 1
+    tx, ty = grid.solve(ssh, form=S.FORM_MIXED)
+    st_tree = grid.stats()
+    grid.tune(tree_passes=0)
+    dx_, dy_ = grid.solve(ssh, form=S.FORM_MIXED)
+    st_direct = grid.stats()
+    ax, ay = grid.solve(ssh, form=S.FORM_ACCURATE)
+    torch.cuda.synchronize()
+    grid.sync()
+    assert st_tree["macs_up_batched"] < 0.5 * st_direct["macs_up_batched"]
+    assert st_tree["macs_down_batched"] < 0.5 * st_direct["macs_down_batched"]
+    assert st_direct["macs_up_batched"] == st_direct["macs_up"]
+    T = lambda a: torch.tensor(a, device="cuda")
+    tg = np.sort(np.random.default_rng(4).choice(g.n, 3000, replace=False)).astype(np.int32)
+    for f in range(4):
+        t = [v[f].cpu().numpy() for v in (tx, ty, dx_, dy_, ax, ay)]
+        assert rel_l2(t[0], t[1], t[2], t[3]) <= 2e-6
+        assert rel_l2(t[0], t[1], t[4], t[5]) <= 5e-6
+        rx, ry = S.direct_sum(T(g.xs), T(g.ys), T(g.zs), T(g.areas * hs[f]), T(tg))
+        assert rel_l2(t[0][tg], t[1][tg], rx.cpu().numpy(), ry.cpu().numpy()) <= 1e-5
+
+
+def test_tune_settings_round_trip_and_keep_accuracy():
+    """Every choice sal_grid_tune_set accepts re-cuts the plan (or the launch
+    shape) and the batched form stays within its bar of the FP64 accurate
+    form; bad settings are refused."""
+    torch = _torch()
+    S, g, hs, grid = _grid("small_20000", 60, 3, seed=8)
+    ssh = torch.tensor(hs, device="cuda")
+    ax, ay = grid.solve(ssh, form=S.FORM_ACCURATE)
+    settings = [dict(chain_ksteps=8), dict(chain_ksteps=64), dict(cta_groups=3), dict(proxy_unit_kpairs=100),
+                dict(tree_passes=0, up_chunk=1000), dict(field_block=32), dict(field_block=64, tree_passes=1)]
+    for ch in settings:
+        now = grid.tune(**ch)
+        for k, v in ch.items():
+            assert now[k] == v
+        mx, my = grid.solve(ssh, form=S.FORM_MIXED)
+        torch.cuda.synchronize()
+        grid.sync()
+        for f in range(3):
+            assert rel_l2(mx[f].cpu().numpy(), my[f].cpu().numpy(), ax[f].cpu().numpy(),
+                          ay[f].cpu().numpy()) <= 5e-6, ch
+    with pytest.raises(S.SalError):
+        grid.tune(chain_ksteps=0)
+    with pytest.raises(S.SalError):
+        grid.tune(field_block=48)
+
+
+def test_autotune_picks_a_setting_within_the_bar():
+    torch = _torch()
+    S, g, hs, grid = _grid("small_20000", 60, 4, seed=12)
+    ssh = torch.tensor(hs, device="cuda")
+    best, ms_best, ms_start = grid.autotune(ssh, ntargets=1000, max_rel_err=5e-6)
+    assert grid.tune() == best
+    assert 0 < ms_best <= ms_start * 1.05
+    mx, my = grid.solve(ssh, form=S.FORM_MIXED)
+    ax, ay = grid.solve(ssh, form=S.FORM_ACCURATE)
+    torch.cuda.synchronize()
+    grid.sync()
+    for f in range(4):
+        assert rel_l2(mx[f].cpu().numpy(), my[f].cpu().numpy(), ax[f].cpu().numpy(), ay[f].cpu().numpy()) <= 5e-6
+    with pytest.raises(S.SalError):
+        grid.autotune(ssh, ntargets=1000, max_rel_err=1e-12)
+    assert grid.tune() == best        # a failed search leaves the setting as it was
