@@ -55,6 +55,8 @@ def _args():
     ap.add_argument("--serve-rate", type=float, default=200.0)
     ap.add_argument("--serve-host", action="store_true", help="serving requests carry host arrays")
     ap.add_argument("--no-serve", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true", help="time the batched form's default settings")
+    ap.add_argument("--no-stt", action="store_true", help="skip the mom6_code.f90 path measurement")
     ap.add_argument("--cpu-table", action="store_true", help="time the oracle on cfg0/cfg1/cfg2 and exit")
     a = ap.parse_args()
     if a.fields is None:
@@ -297,6 +299,104 @@ def cpu_table(args):
     print(json.dumps({"cpu_table": rows, "kind": "port", "cores": cores}), flush=True)
 
 
+def stt_run(args, S, torch, dev):
+    """The mom6_code.f90 path (single tree traversal) on the 0.25 degree
+    1440 x 720 lon-lat ocean grid (cfg1), plain FP64 in the reference's
+    operation order (ref_compat weights): device time of one solve
+    (proxy_source_compute + pc_compute + pp_compute as one sal_solve on the
+    grid), and end to end through the reference-signature entry points with
+    host arrays, as mom6_code.f90:272-312 calls them (the first call builds
+    and caches the device grids; the timed calls reuse them).  The oracle's
+    time on the host's cores for the same three calls comes from a bounded
+    sample of targets."""
+    from salgpu import synth
+    g = synth.config_grid("cfg1", device=dev)
+    h = synth.config_ssh("cfg1", g, nfields=1, seed=13, device=dev)[0]
+    t0 = time.perf_counter()
+    tree = S.tree_traverse(g.xs, g.ys, g.zs, g.n, 200)
+    ppan = S.assign_points_to_panels(tree, g.xs, g.ys, g.zs)
+    pc, pp = S.single_tree_traversal(tree, 0.7, 200, g.xs, g.ys, g.zs)
+    t_lists = time.perf_counter() - t0
+    grid = S.mom6_grid(tree, pc, pp, g.xs, g.ys, g.zs, g.areas, 8, ref_compat=True, device=dev.index or 0)
+    ssh = torch.tensor(h, device=dev)
+    out = (torch.empty_like(ssh), torch.empty_like(ssh))
+    for _ in range(2):
+        grid.solve(ssh, out=out)
+    stream = torch.cuda.current_stream(dev)
+    e = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    e[0].record(stream)
+    for _ in range(5):
+        grid.solve(ssh, out=out)
+    e[1].record(stream)
+    torch.cuda.synchronize()
+    dev_ms = e[0].elapsed_time(e[1]) / 5
+    grid.timing(1)
+    for _ in range(3):
+        grid.solve(ssh, out=out)
+    phase, nsol = grid.timing(0)
+    st = grid.stats()
+    del grid
+    # end to end: the three reference-signature calls on host arrays
+    P = (8 + 1) ** 2
+    npn = tree.npanels
+    w = np.zeros(P * npn)
+    sx, sy = np.zeros(g.n), np.zeros(g.n)
+    S.dropin_config(S.FORM_REF, S.MODE_STT_REF_COMPAT)
+    t0 = time.perf_counter()
+    S.proxy_source_compute(w, tree, ppan, g.xs, g.ys, g.zs, h, g.areas, 8, g.n)
+    S.pc_compute(sx, sy, pc, tree, g.xs, g.ys, g.zs, 8, w)
+    S.pp_compute(sx, sy, pp, tree, g.xs, g.ys, g.zs, g.areas, h)
+    first = time.perf_counter() - t0
+    reps = []
+    for _ in range(3):
+        w[:] = 0.0
+        sx[:] = 0.0
+        sy[:] = 0.0
+        t0 = time.perf_counter()
+        S.proxy_source_compute(w, tree, ppan, g.xs, g.ys, g.zs, h, g.areas, 8, g.n)
+        S.pc_compute(sx, sy, pc, tree, g.xs, g.ys, g.zs, 8, w)
+        S.pp_compute(sx, sy, pp, tree, g.xs, g.ys, g.zs, g.areas, h)
+        reps.append(time.perf_counter() - t0)
+    S.dropin_release()
+    e2e_s = float(np.median(reps))
+    pairs = st["pairs_pp"] + st["pairs_pc"]
+    out = {"workload": f"cfg1: {g.n} lon-lat ocean cells (1440 x 720 before the mask), single tree traversal "
+                       "(mom6_code.f90), d=8, theta=0.7, leaf<200, plain FP64, ref_compat weights",
+           "cells": g.n, "pc_entries": len(pc), "pp_entries": len(pp), "kernel_pairs": pairs,
+           "device_ms": dev_ms, "evals_per_s": g.n / (dev_ms * 1e-3),
+           "passes_ms": {"prep_upward": phase[0] / nsol, "leaf_pc_pp": phase[2] / nsol},
+           "fp64_tflops_leaf": FLOPS_PER_PAIR * pairs / (phase[2] / nsol * 1e-3) / 1e12,
+           "e2e": {"value": g.n / e2e_s, "unit": "evals/s", "seconds": e2e_s, "first_call_s": first,
+                   "api": "sal_mom6_proxy_source_compute + sal_mom6_pc_compute + sal_mom6_pp_compute, host arrays"},
+           "setup_s": {"tree_and_lists": t_lists, "plan_and_upload": st["setup_seconds"]}}
+    if not args.no_cpu:
+        # the oracle's three calls on every list entry of a seeded target
+        # sample, all host threads; the solve time scales by the sampled share
+        # of the entries
+        from oracle import oracle as O
+        cores = os.cpu_count() or 1
+        ot = O.tree_traverse(g.xs, g.ys, g.zs, 200)
+        opan = O.assign_points_to_panels(ot, g.xs, g.ys, g.zs)
+        t0 = time.perf_counter()
+        wr = O.proxy_source_compute(ot, opan, g.xs, g.ys, g.zs, h, g.areas, 8, True, nthreads=cores)
+        t_up = time.perf_counter() - t0
+        tg = np.sort(np.random.default_rng(21).choice(g.n, 60000, replace=False))
+        sel = np.zeros(g.n + 1, bool)
+        sel[tg + 1] = True
+        spc, spp = pc[sel[pc[:, 0]]], pp[sel[pp[:, 0]]]
+        t0 = time.perf_counter()
+        O.pc_compute(ot, spc, g.xs, g.ys, g.zs, 8, wr, nthreads=cores)
+        O.pp_compute(ot, spp, g.xs, g.ys, g.zs, g.areas, h, nthreads=cores)
+        t_s = time.perf_counter() - t0
+        frac = (len(spc) * P + len(spp)) / (len(pc) * P + len(pp))
+        cpu_s = t_up + t_s / frac
+        out["cpu_baseline"] = {"value": g.n / cpu_s, "unit": "evals/s", "cores": cores, "kind": "port",
+                               "sample": f"proxy_source_compute whole ({t_up:.1f} s); pc/pp_compute on the "
+                                         f"entries of 60,000 seeded targets ({100 * frac:.1f}% of the work, "
+                                         f"{t_s:.1f} s), scaled to the whole list"}
+    return out
+
+
 def serving_run(args, S, torch, dev):
     """The serving mix: four Fibonacci ocean grids (40,962 / 163,842 / 655,362
     / 2,313,486 cells) resident under an HBM budget, Poisson arrivals at
@@ -406,6 +506,16 @@ def main():
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)   # > 126 MB L2
     stream = torch.cuda.current_stream(dev)
 
+    tuned = None
+    if form == S.FORM_MIXED and not args.no_autotune:
+        # the batched form's autotuner on this grid and these fields: coordinate
+        # descent over its choices, each timed with the L2 flushed and checked
+        # against the FP64 direct sum (first field, 2,000 targets, 5e-6 bar)
+        default = grid.tune()
+        t0 = time.perf_counter()
+        best, ms_best, ms_default = grid.autotune(ssh[:64], ntargets=2000, max_rel_err=5e-6)
+        tuned = {"default": default, "chosen": best, "ms_default": ms_default, "ms_chosen": ms_best,
+                 "search_s": time.perf_counter() - t0}
     for _ in range(args.warmup):
         grid.solve(ssh, form=form, out=(ox, oy))
     torch.cuda.synchronize()
@@ -434,6 +544,7 @@ def main():
         grid.solve(ssh, form=form, out=(ox, oy))
     phase, nsol = grid.timing(0)
     up_ms, proxy_ms, leaf_ms = (phase[i] / nsol for i in range(3))
+    st = grid.stats()
     if form == S.FORM_MIXED:                     # one timing record per field block
         nblk = (F + 63) // 64 if F > 32 else 1
         up_ms, proxy_ms, leaf_ms = up_ms * nblk, proxy_ms * nblk, leaf_ms * nblk
@@ -504,7 +615,7 @@ def main():
             pass
         bf16 = peaks.get("bf16_tflops", 1590.0)
         peak = bf16 / 2.0          # dense TF32 = half the bf16 rate
-        leaf_flops = 4.0 * F * (st["pairs_pp"] + st["pairs_pc"] + 3.0 * st["macs_down"])
+        leaf_flops = 4.0 * F * (st["pairs_pp"] + st["pairs_pc"] + 3.0 * st["macs_down_batched"])
         achieved = leaf_flops / (leaf_ms * 1e-3) / 1e12
         roof = {"bound": "tensor", "kernel": "tc_leaf_kernel<0> (tcgen05 TF32 hi/lo, M=128 field parts x N=256 target "
                           "components; PP+PC kernel tiles, DOWN interpolation) + split_store_kernel (potentials)",
@@ -530,6 +641,9 @@ def main():
     cb = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cb = cpu_baseline(args, g, h[0], args.cpu_seconds)
+    stt = None
+    if rank == 0 and world == 1 and form == S.FORM_MIXED and not args.no_stt:
+        stt = stt_run(args, S, torch, dev)
     served = None
     if rank == 0 and world == 1 and form == S.FORM_MIXED and not args.no_serve:
         del grid
@@ -553,7 +667,9 @@ def main():
                 "e2e": {"value": plain_e2e, "unit": "evals/s", "api": "sal_solve_host, SAL_FORM_REF, one field",
                         "h2d_bytes_per_step": 8 * g.n, "d2h_bytes_per_step": 16 * g.n}},
             "roofline": roof,
-            "work": {k: st[k] for k in ("pairs_pp", "pairs_pc", "pairs_cp", "pairs_cc", "macs_up", "macs_down")},
+            "work": {k: st[k] for k in ("pairs_pp", "pairs_pc", "pairs_cp", "pairs_cc", "macs_up", "macs_down",
+                                        "macs_up_batched", "macs_down_batched")},
+            "autotune": tuned,
             "setup_s": {"grid_generation": t_gen, "tree_and_lists": t_lists, "plan_and_upload": st["setup_seconds"]},
             "e2e": {"value": e2e_val, "unit": "evals/s", "h2d_bytes_per_step": 8 * g.n * F,
                     "d2h_bytes_per_step": 16 * g.n * F, "steps": e2e_steps,
@@ -566,6 +682,8 @@ def main():
         }
         if cb:
             line["cpu_baseline"] = cb
+        if stt:
+            line["stt_mom6"] = stt
         if served:
             line["serving"] = served
         print(json.dumps(line), flush=True)

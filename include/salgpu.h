@@ -321,6 +321,16 @@ int sal_dropin_config(int32_t form, int32_t mom6_mode);
 /* Frees every grid the four entry points above keep. */
 int sal_dropin_release(void);
 
+/* ------------------------------------------------------------------ grid ingestion
+ * code.f90:36-56 (and mom6_code.f90:95-117) read five files of point_count
+ * values, one per line, with list-directed READs.  sal_read_values reads the
+ * first count values of such a file (E, D or Q exponents, blank lines
+ * skipped) with every host thread, or, for a name ending in ".f64", count
+ * raw little-endian float64 values as sal_write_values writes them.  Fewer
+ * values than count, or a line that is not a number, returns SAL_EINVAL. */
+int sal_read_values(const char *path, int64_t count, double *out);
+int sal_write_values(const char *path, int64_t count, const double *values);
+
 /* FP64 direct O(N^2) sum at nt targets (0-based indices into the sources),
  * with the reference kernel in its own operation order.  Device pointers;
  * w = area * ssh per source.  Overwrites out_x/out_y (nt each). */

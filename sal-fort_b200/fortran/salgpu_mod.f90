@@ -28,7 +28,7 @@ MODULE SALGPU_MOD
     use tree_module, only: cube_panel, interaction_pair
     implicit none
     private
-    public :: fast_sum, proxy_source_compute, pc_compute, pp_compute
+    public :: fast_sum, proxy_source_compute, pc_compute, pp_compute, salgpu_read
 
     integer(c_int), parameter :: SAL_OK = 0, SAL_ETREE = -6
 
@@ -80,6 +80,12 @@ MODULE SALGPU_MOD
         integer(c_int) function sal_dropin_config(form, mom6_mode) bind(C, name="sal_dropin_config")
             import :: c_int, c_int32_t
             integer(c_int32_t), value :: form, mom6_mode
+        end function
+        integer(c_int) function sal_read_values(path, count, out) bind(C, name="sal_read_values")
+            import :: c_int, c_int64_t, c_double, c_char
+            character(kind=c_char), intent(in) :: path(*)
+            integer(c_int64_t), value :: count
+            real(c_double), intent(out) :: out(*)
         end function
         type(c_ptr) function sal_last_error() bind(C, name="sal_last_error")
             import :: c_ptr
@@ -166,6 +172,16 @@ MODULE SALGPU_MOD
             flat(width*(i-1)+2) = list(i)%index_source
             IF (width == 3) flat(width*i) = list(i)%interact_type
         END DO
+    END SUBROUTINE
+
+    ! Reads the first size(values) values of a one-value-per-line input file
+    ! (or of its raw ".f64" form) with every host thread, in place of the
+    ! drivers' list-directed read loops (code.f90:36-56):
+    !     call salgpu_read('data-files/2313486_mpas_grid_x.csv', xs)
+    SUBROUTINE salgpu_read(path, values)
+        character(len=*), intent(in) :: path
+        real(8), intent(out) :: values(:)
+        call check(sal_read_values(trim(path)//c_null_char, int(size(values), c_int64_t), values))
     END SUBROUTINE
 
     ! fast_sum_module.f90:291-332, same arguments.

@@ -39,7 +39,8 @@ EXPORTS = (
     "sal_grid_timing", "sal_fma_peak", "sal_direct_sum_noalloc", "sal_solve_host", "sal_solve_host_async",
     "sal_solve_host_wait", "sal_grid_set_graphs", "sal_grid_inject_timeout", "sal_fast_sum",
     "sal_mom6_proxy_source_compute", "sal_mom6_pc_compute", "sal_mom6_pp_compute", "sal_dropin_config",
-    "sal_dropin_release", "sal_grid_tune_get", "sal_grid_tune_set", "sal_grid_autotune",
+    "sal_dropin_release", "sal_grid_tune_get", "sal_grid_tune_set", "sal_grid_autotune", "sal_read_values",
+    "sal_write_values",
 )
 
 
@@ -136,6 +137,8 @@ def lib():
         L.sal_mom6_pp_compute.argtypes = [vp, vp, vp, i64, i32, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp,
                                           vp, vp, i32, i32]
         L.sal_dropin_config.argtypes = [i32, i32]
+        L.sal_read_values.argtypes = [C.c_char_p, i64, vp]
+        L.sal_write_values.argtypes = [C.c_char_p, i64, vp]
         L.sal_grid_tune_get.argtypes = [vp, C.POINTER(Tune)]
         L.sal_grid_tune_set.argtypes = [vp, C.POINTER(Tune)]
         L.sal_grid_autotune.argtypes = [vp, vp, i32, i64, i32, d, C.POINTER(Tune), C.POINTER(d), C.POINTER(d)]
@@ -400,6 +403,20 @@ class Grid:
 
     def pp_compute_host(self, sshs, sal_x, sal_y):
         _check(lib().sal_pp_compute_host(self.handle, _ptr(_f64(sshs)), _ptr(sal_x), _ptr(sal_y)))
+
+
+def read_values(path, count) -> np.ndarray:
+    """The first count values of a one-value-per-line file (the reference's
+    input CSVs, code.f90:36-56) or of a raw float64 ".f64" file."""
+    out = np.empty(int(count), np.float64)
+    _check(lib().sal_read_values(os.fsencode(path), int(count), _ptr(out)))
+    return out
+
+
+def write_values(path, values):
+    """Writes values as raw little-endian float64 (the ".f64" form)."""
+    v = _f64(values)
+    _check(lib().sal_write_values(os.fsencode(path), len(v), _ptr(v)))
 
 
 def fma_peak(precision=64) -> float:

@@ -163,3 +163,40 @@ def test_reference_signature_entry_points_check_their_arguments_on_the_host():
         S.fast_sum(lon, lat, L, panels, xs2, ys2, g.zs, g.areas, hh[0], g.n, 8, with_points_inside=False)
     assert e.value.code == S.SAL_ETREE
     assert not lon.any() and not lat.any()
+
+
+def test_grid_ingestion_reads_list_directed_files_and_raw_float64(tmp_path):
+    """sal_read_values parses one-value-per-line files as the reference's
+    drivers read them (code.f90:36-56): Fortran list-directed forms with E, D
+    or a bare-sign exponent, blank lines, trailing blanks; every value comes
+    back bit for bit.  The raw .f64 form round-trips; short files and bad
+    lines are refused."""
+    import salgpu as S
+    rng = np.random.default_rng(5)
+    v = np.concatenate([rng.standard_normal(5000) * 10.0 ** rng.integers(-300, 300, 5000), [0.0, -0.0, 1.0, -2.5]])
+    # %.17g round-trips every double; add Fortran-style renderings
+    lines = [f"  {x:.17g}   " for x in v]
+    lines[1] = lines[1].replace("e", "D")
+    lines[2] = " " + repr(float(v[2])).upper() + "\r"
+    lines.insert(7, "")
+    p = tmp_path / "x.csv"
+    p.write_text("\n".join(lines) + "\n")
+    out = S.read_values(str(p), len(v))
+    assert np.array_equal(out.view(np.uint64), v.view(np.uint64))
+    assert np.array_equal(S.read_values(str(p), 10), v[:10])
+    q = tmp_path / "y.csv"
+    q.write_text("  0.125-002\n 1.5D+3\n -2.0E-1\n")
+    assert np.array_equal(S.read_values(str(q), 3), [0.125e-2, 1.5e3, -0.2])
+    b = tmp_path / "x.f64"
+    S.write_values(str(b), v)
+    assert np.array_equal(S.read_values(str(b), len(v)).view(np.uint64), v.view(np.uint64))
+    with pytest.raises(S.SalError) as e:
+        S.read_values(str(p), len(v) + 1)
+    assert e.value.code == S.SAL_EINVAL and "fewer" in str(e.value)
+    r = tmp_path / "bad.csv"
+    r.write_text("1.0\nabc\n3.0\n")
+    with pytest.raises(S.SalError) as e:
+        S.read_values(str(r), 3)
+    assert "value 2" in str(e.value)
+    with pytest.raises(S.SalError):
+        S.read_values(str(tmp_path / "missing.csv"), 1)
