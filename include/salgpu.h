@@ -218,6 +218,21 @@ int sal_grid_destroy(sal_grid *g);
 int sal_solve(sal_grid *g, const double *ssh, int32_t nfields, int64_t ld_ssh, double *out_x, double *out_y,
               int64_t ld_out, int32_t form, void *stream);
 
+/* Batched solves of several grids whose leaf passes share one launch (no
+ * counterpart in the reference): the grids' smaller passes run one after
+ * another on stream, then one tcgen05 leaf pass walks the target groups of
+ * all of them, so grids of uneven size fill the GPU together instead of each
+ * leaving it idle at its launch's tail.  SAL_FORM_MIXED; per grid k, nfields[k]
+ * (1..64) fields at ssh[k] (column f at ssh[k] + f * ld_ssh[k]) and outputs at
+ * out_x[k] / out_y[k] (leading dimension ld_out[k]).  At most 8 distinct
+ * SAL_MODE_DTT grids of one device and one degree, each created with
+ * max_fields > 32.  Results equal those of separate sal_solve calls bit for
+ * bit.  A device-side time-out is reported by sal_grid_sync of grids[0].
+ * Asynchronous on stream; a caller may capture it into a CUDA graph. */
+int sal_solve_joint(sal_grid *const *grids, int32_t ngrids, const double *const *ssh, const int32_t *nfields,
+                    const int64_t *ld_ssh, double *const *out_x, double *const *out_y, const int64_t *ld_out,
+                    void *stream);
+
 /* sal_solve on host buffers: copies the fields to the device, solves, copies
  * both components back and waits (outputs overwritten).  Device staging is
  * allocated on the first call and kept by the grid. */

@@ -560,13 +560,40 @@ static int ensure_mixed(GridImpl &g, int FT) {
     return SAL_OK;
 }
 
+// Arguments of the tcgen05 leaf pass of one 64-field block.
+static mix::TcArgs leaf_args(GridImpl &g, double *ox, double *oy, int64_t ld_out, int f0, int nf) {
+    const Plan &pl = g.plan;
+    mix::TcArgs t{};
+    t.groups = g.tc_leaf_groups;
+    t.ngroups = (int)pl.tc_leaf_groups.size();
+    t.items = g.tc_items;
+    t.sxyz = g.sxyz;
+    t.bstore = g.bstore;
+    t.tgt = g.pool;
+    t.xieta = g.xieta;
+    t.tgt_nodes = g.tc_down_nodes;
+    t.selfk = g.selfk;
+    t.wF = g.wF;
+    t.perm = g.perm;
+    t.d = pl.d;
+    t.P = pl.P;
+    t.out_x = ox;
+    t.out_y = oy;
+    t.ld_out = ld_out;
+    t.f0 = f0;
+    t.nf = nf;
+    return t;
+}
+
 // One block of up to FT fields in the batched form: per-field weights, upward
-// pass, proxy potentials, leaf pass (six launches).
+// pass, proxy potentials, leaf pass.  With joint != NULL (tcgen05 blocks) the
+// leaf pass is not launched: its arguments go to *joint.
 static void solve_mixed_block(GridImpl &g, const double *ssh, int64_t ld_ssh, int f0, int nf, double *ox, double *oy,
-                              int64_t ld_out, cudaStream_t st) {
+                              int64_t ld_out, cudaStream_t st, mix::TcArgs *joint = nullptr) {
     const Plan &pl = g.plan;
     const int n = pl.n, P = pl.P, FT = g.FT;
-    if (g.timing) cudaEventRecord(g.ev[0], st);
+    const bool timed = g.timing && !joint;   // a joint solve's leaf pass is not this grid's alone
+    if (timed) cudaEventRecord(g.ev[0], st);
     mix::launch_prep_mix(g.area, ssh, ld_ssh, g.iperm, n, f0, nf, FT, g.wF, st);
     mix::MixArgs a{};
     a.pool = g.pool;
@@ -619,7 +646,7 @@ static void solve_mixed_block(GridImpl &g, const double *ssh, int64_t ld_ssh, in
         mix::launch_mix(2, FT, u, (int)pl.mix_up_groups.size(), st);
         mix::launch_finalize_mix(g.up_unit_beg, g.mix_up_partial, g.nsrc, P, FT, g.wF + (size_t)n * FT, st);
     }
-    if (g.timing) cudaEventRecord(g.ev[1], st);
+    if (timed) cudaEventRecord(g.ev[1], st);
     // 64-field blocks: the proxy pass on tcgen05
     if (g.bstore && !pl.tc_proxy_groups.empty()) {
         mix::TcArgs p{};
@@ -647,7 +674,14 @@ static void solve_mixed_block(GridImpl &g, const double *ssh, int64_t ld_ssh, in
         mix::launch_mix(1, FT, q, (int)pl.mix_proxy_groups.size(), st);
         mix::launch_finalize_mix(g.proxy_unit_beg, g.mix_proxy_partial, g.ntgt, 3 * P, FT, g.phiF, st);
     }
-    if (g.timing) cudaEventRecord(g.ev[2], st);
+    if (timed) cudaEventRecord(g.ev[2], st);
+    if (joint) {
+        // the potential rows of the split weight store; the caller runs the
+        // leaf pass, jointly with other grids'
+        mix::launch_split_store(g.bsrc, pl.tc_src_ksteps, (int64_t)pl.bsrc.size() / 8, g.wF, g.phiF, g.bstore, st);
+        *joint = leaf_args(g, ox, oy, ld_out, f0, nf);
+        return;
+    }
     a.items = g.mix_leaf_items;
     a.tgt = g.pool;
     a.tgt_nodes = g.tgt_nodes;
@@ -655,31 +689,12 @@ static void solve_mixed_block(GridImpl &g, const double *ssh, int64_t ld_ssh, in
         // 64-field blocks: the potential rows of the split weight store, then
         // the tcgen05 leaf pass
         mix::launch_split_store(g.bsrc, pl.tc_src_ksteps, (int64_t)pl.bsrc.size() / 8, g.wF, g.phiF, g.bstore, st);
-        mix::TcArgs t{};
-        t.groups = g.tc_leaf_groups;
-        t.ngroups = (int)pl.tc_leaf_groups.size();
-        t.items = g.tc_items;
-        t.sxyz = g.sxyz;
-        t.bstore = g.bstore;
-        t.tgt = g.pool;
-        t.xieta = g.xieta;
-        t.tgt_nodes = g.tc_down_nodes;
-        t.selfk = g.selfk;
-        t.wF = g.wF;
-        t.perm = g.perm;
-        t.d = pl.d;
-        t.P = P;
-        t.out_x = ox;
-        t.out_y = oy;
-        t.ld_out = ld_out;
-        t.f0 = f0;
-        t.nf = nf;
-        mix::launch_tc_leaf(t, g.nsm, cg, g.err, st);
+        mix::launch_tc_leaf(leaf_args(g, ox, oy, ld_out, f0, nf), g.nsm, cg, g.err, st);
     } else {
         a.groups = g.mix_leaf_groups;
         mix::launch_mix(0, FT, a, (int)pl.mix_leaf_groups.size(), st);
     }
-    if (g.timing) {
+    if (timed) {
         cudaEventRecord(g.ev[3], st);
         cudaEventSynchronize(g.ev[3]);
         float t01 = 0, t12 = 0, t23 = 0;
@@ -721,6 +736,41 @@ static int capture_mixed(GridImpl &g, const GridImpl::GraphShape &k, cudaStream_
         g.graphs.erase(g.graphs.begin());
     }
     g.graphs.push_back({k, exec});
+    return SAL_OK;
+}
+
+extern "C" int sal_solve_joint(sal_grid *const *grids, int32_t ngrids, const double *const *ssh,
+                               const int32_t *nfields, const int64_t *ld_ssh, double *const *out_x,
+                               double *const *out_y, const int64_t *ld_out, void *stream) {
+    if (!grids || !ssh || !nfields || !ld_ssh || !out_x || !out_y || !ld_out) return set_error(SAL_EINVAL, "null argument");
+    if (ngrids < 1 || ngrids > mix::kMaxJoint)
+        return set_error(SAL_EINVAL, "ngrids must be in 1.." + std::to_string(mix::kMaxJoint));
+    cudaStream_t st = (cudaStream_t)stream;
+    mix::TcArgs args[mix::kMaxJoint];
+    for (int k = 0; k < ngrids; ++k) {
+        if (!grids[k] || !ssh[k] || !out_x[k] || !out_y[k]) return set_error(SAL_EINVAL, "null argument");
+        for (int j = 0; j < k; ++j)
+            if (grids[j] == grids[k]) return set_error(SAL_EINVAL, "a grid appears twice in a joint solve");
+        GridImpl &g = grids[k]->g;
+        if (g.plan.mode != SAL_MODE_DTT) return set_error(SAL_EINVAL, "the batched form needs a SAL_MODE_DTT grid");
+        if (nfields[k] < 1 || nfields[k] > 64) return set_error(SAL_EINVAL, "a joint solve takes 1..64 fields per grid");
+        if (nfields[k] > 1 && (ld_ssh[k] < g.plan.n || ld_out[k] < g.plan.n))
+            return set_error(SAL_EINVAL, "leading dimension < point_count");
+        if (g.dev != grids[0]->g.dev || g.plan.d != grids[0]->g.plan.d)
+            return set_error(SAL_EINVAL, "the grids of a joint solve share one device and one degree");
+        if (g.max_fields <= 32 || g.plan.tc_items.empty())
+            return set_error(SAL_EINVAL, "a joint solve needs grids with 64-field blocks (max_fields > 32)");
+    }
+    CK(cudaSetDevice(grids[0]->g.dev));
+    for (int k = 0; k < ngrids; ++k) {
+        GridImpl &g = grids[k]->g;
+        int rc = ensure_mixed(g, 64);
+        if (rc) return rc;
+        solve_mixed_block(g, ssh[k], ld_ssh[k], 0, nfields[k], out_x[k], out_y[k], ld_out[k], st, &args[k]);
+    }
+    GridImpl &g0 = grids[0]->g;
+    mix::launch_tc_leaf_joint(args, ngrids, g0.nsm, g0.plan.tc_opt.cta_groups, g0.err, st);
+    CK(cudaGetLastError());
     return SAL_OK;
 }
 

@@ -69,7 +69,15 @@ struct TcArgs {
 };
 // cta_groups: groups one CTA walks at most (the grid has every SM busy
 // otherwise)
+// Arguments of a leaf pass over several grids in one launch (same degree).
+constexpr int kMaxJoint = 8;
+struct TcJoint {
+    TcArgs g[kMaxJoint];
+    int32_t beg[kMaxJoint + 1];   // first joint group of each grid; beg[ngrids] = all groups
+    int32_t ngrids;
+};
 void launch_tc_leaf(const TcArgs &a, int nsm, int cta_groups, int *err, cudaStream_t st);
+void launch_tc_leaf_joint(const TcArgs *grids, int ngrids, int nsm, int cta_groups, int *err, cudaStream_t st);
 void launch_tc_proxy(const TcArgs &a, int nsm, int cta_groups, int *err, cudaStream_t st);
 void launch_tc_upward(const TcArgs &a, int nsm, int cta_groups, int *err, cudaStream_t st);
 void launch_basis_store(const int32_t *bas, int64_t nbk, const double2 *xieta, const double *src_nodes, int n,

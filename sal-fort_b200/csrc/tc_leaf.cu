@@ -302,12 +302,23 @@ __device__ __noinline__ void fold_chain(uint32_t td, int q, int lane, bool end, 
     if (!end) tmem_wait_st();
 }
 
-template <int MODE>
-__global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(TcArgs a, int *err) {
+// JOINT: one launch over the groups of several grids (of one degree): group
+// gi belongs to the grid k with J.beg[k] <= gi < J.beg[k + 1] and carries
+// that grid's arguments.  Otherwise J.g[0] is the only grid.
+template <int MODE, bool JOINT>
+__global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(const __grid_constant__ TcJoint J, int *err) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     TcSmem &sm = *reinterpret_cast<TcSmem *>(smem_raw);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int n = a.d + 1, P = a.P;
+    const int n = J.g[0].d + 1, P = J.g[0].P;
+    const int total = JOINT ? J.beg[J.ngrids] : J.g[0].ngroups;
+    // the grid of joint group gi
+    auto grid_of = [&](int gi) -> int {
+        int k = 0;
+        if (JOINT)
+            while (k + 1 < J.ngrids && gi >= J.beg[k + 1]) ++k;
+        return k;
+    };
     volatile int *abort = &sm.abort;
 
     // ------------------------------------------------------------ set-up
@@ -359,8 +370,10 @@ __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(TcArgs a, int *err
         // stage's weights: the loader warp copies them up to kWStages stages
         // ahead, so no global-memory latency sits in a producer task.
 
-        for (int gi = blockIdx.x; gi < a.ngroups; gi += gridDim.x) {
-            const MixGroup G = a.groups[gi];
+        for (int gi = blockIdx.x; gi < total; gi += gridDim.x) {
+            const int gk = grid_of(gi);
+            const TcArgs &a = J.g[gk];
+            const MixGroup G = a.groups[gi - J.beg[gk]];
             const int ni = G.ie - G.ib;
             const int rb = (G.nt + 31) >> 5;
             const int wb = rb >= 3 ? (warp & 3) : rb == 2 ? (warp & 1) : 0;            // row block
@@ -590,8 +603,10 @@ __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(TcArgs a, int *err
         // ============================================================ MMA issue
         uint32_t cc = 0;           // chains started
         bool chain_open = false;
-        for (int gi = blockIdx.x; gi < a.ngroups; gi += gridDim.x) {
-            const MixGroup G = a.groups[gi];
+        for (int gi = blockIdx.x; gi < total; gi += gridDim.x) {
+            const int gk = grid_of(gi);
+            const TcArgs &a = J.g[gk];
+            const MixGroup G = a.groups[gi - J.beg[gk]];
             TcItem nxt = G.ib < G.ie ? a.items[G.ib] : TcItem{};
             for (int k = G.ib; k < G.ie; ++k) {
                 const TcItem it = nxt;
@@ -637,8 +652,10 @@ __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(TcArgs a, int *err
         __syncwarp();
     } else if (warp == kLoadWarp) {
         // ============================================================ loads
-        for (int gi = blockIdx.x; gi < a.ngroups; gi += gridDim.x) {
-            const MixGroup G = a.groups[gi];
+        for (int gi = blockIdx.x; gi < total; gi += gridDim.x) {
+            const int gk = grid_of(gi);
+            const TcArgs &a = J.g[gk];
+            const MixGroup G = a.groups[gi - J.beg[gk]];
             TcItem nxt = G.ib < G.ie ? a.items[G.ib] : TcItem{};
             for (int k = G.ib; k < G.ie; ++k) {
                 const TcItem it = nxt;
@@ -683,8 +700,10 @@ __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(TcArgs a, int *err
         const int q = warp & 3;
         const uint32_t tq = tmem + ((uint32_t)(32 * q) << 16);
         uint32_t cc = 0;   // chains folded
-        for (int gi = blockIdx.x; gi < a.ngroups; gi += gridDim.x) {
-            const MixGroup G = a.groups[gi];
+        for (int gi = blockIdx.x; gi < total; gi += gridDim.x) {
+            const int gk = grid_of(gi);
+            const TcArgs &a = J.g[gk];
+            const MixGroup G = a.groups[gi - J.beg[gk]];
             bool first = true;
             for (int k = G.ib; k < G.ie; ++k) {
                 if (!(a.items[k].kind & kTcFlush)) continue;
@@ -811,19 +830,41 @@ size_t tc_smem_bytes() {
     return need > 120 * 1024 ? need : 120 * 1024;
 }
 
-template <int MODE>
-static void launch_tc(const TcArgs &a, int nsm, int cta_groups, int *err, cudaStream_t st) {
-    if (a.ngroups <= 0) return;
+template <int MODE, bool JOINT>
+static void launch_tc(const TcJoint &J, int nsm, int cta_groups, int *err, cudaStream_t st) {
+    const int total = J.beg[J.ngrids];
+    if (total <= 0) return;
     const size_t smem = tc_smem_bytes();
     static std::atomic<unsigned long long> done{0};
-    smem_attr_once((const void *)tc_leaf_kernel<MODE>, (int)smem, done);
+    smem_attr_once((const void *)tc_leaf_kernel<MODE, JOINT>, (int)smem, done);
     // every SM busy, but no CTA longer than cta_groups groups: with short
     // CTAs, kernels of other streams (higher-priority grids) get SMs as CTAs
     // retire
     const int per = cta_groups > 0 ? cta_groups : 1;
-    int grid = (a.ngroups + per - 1) / per;
-    if (grid < nsm) grid = a.ngroups < nsm ? a.ngroups : nsm;
-    tc_leaf_kernel<MODE><<<grid, kThreads, smem, st>>>(a, err);
+    int grid = (total + per - 1) / per;
+    if (grid < nsm) grid = total < nsm ? total : nsm;
+    tc_leaf_kernel<MODE, JOINT><<<grid, kThreads, smem, st>>>(J, err);
+}
+
+template <int MODE>
+static void launch_tc(const TcArgs &a, int nsm, int cta_groups, int *err, cudaStream_t st) {
+    TcJoint J{};
+    J.g[0] = a;
+    J.ngrids = 1;
+    J.beg[0] = 0;
+    J.beg[1] = a.ngroups;
+    launch_tc<MODE, false>(J, nsm, cta_groups, err, st);
+}
+
+void launch_tc_leaf_joint(const TcArgs *grids, int ngrids, int nsm, int cta_groups, int *err, cudaStream_t st) {
+    TcJoint J{};
+    J.ngrids = ngrids;
+    J.beg[0] = 0;
+    for (int k = 0; k < ngrids; ++k) {
+        J.g[k] = grids[k];
+        J.beg[k + 1] = J.beg[k] + grids[k].ngroups;
+    }
+    launch_tc<0, true>(J, nsm, cta_groups, err, st);
 }
 
 void launch_tc_leaf(const TcArgs &a, int nsm, int cg, int *err, cudaStream_t st) { launch_tc<0>(a, nsm, cg, err, st); }

@@ -40,7 +40,7 @@ EXPORTS = (
     "sal_solve_host_wait", "sal_grid_set_graphs", "sal_grid_inject_timeout", "sal_fast_sum",
     "sal_mom6_proxy_source_compute", "sal_mom6_pc_compute", "sal_mom6_pp_compute", "sal_dropin_config",
     "sal_dropin_release", "sal_grid_tune_get", "sal_grid_tune_set", "sal_grid_autotune", "sal_read_values",
-    "sal_write_values",
+    "sal_write_values", "sal_solve_joint",
 )
 
 
@@ -138,6 +138,7 @@ def lib():
                                           vp, vp, i32, i32]
         L.sal_dropin_config.argtypes = [i32, i32]
         L.sal_read_values.argtypes = [C.c_char_p, i64, vp]
+        L.sal_solve_joint.argtypes = [vp, i32, vp, vp, vp, vp, vp, vp, vp]
         L.sal_write_values.argtypes = [C.c_char_p, i64, vp]
         L.sal_grid_tune_get.argtypes = [vp, C.POINTER(Tune)]
         L.sal_grid_tune_set.argtypes = [vp, C.POINTER(Tune)]
@@ -403,6 +404,28 @@ class Grid:
 
     def pp_compute_host(self, sshs, sal_x, sal_y):
         _check(lib().sal_pp_compute_host(self.handle, _ptr(_f64(sshs)), _ptr(sal_x), _ptr(sal_y)))
+
+
+def solve_joint(grids, sshs, outs=None, stream=None):
+    """Batched solves of several grids with one shared leaf-pass launch
+    (sal_solve_joint).  grids: Grid objects (max_fields > 32, one degree);
+    sshs: (F_k, N_k) float64 CUDA tensors, F_k <= 64.  Returns the list of
+    (out_x, out_y) per grid."""
+    import torch
+    k = len(grids)
+    sshs = [s.reshape(-1, g.n).contiguous() for s, g in zip(sshs, grids)]
+    if outs is None:
+        outs = [(torch.empty_like(s), torch.empty_like(s)) for s in sshs]
+    P = C.c_void_p * k
+    gh = P(*[g.handle.value for g in grids])
+    sp = P(*[s.data_ptr() for s in sshs])
+    xp = P(*[o[0].data_ptr() for o in outs])
+    yp = P(*[o[1].data_ptr() for o in outs])
+    nf = (C.c_int32 * k)(*[s.shape[0] for s in sshs])
+    ld = (C.c_int64 * k)(*[g.n for g in grids])
+    st = stream if stream is not None else torch.cuda.current_stream(sshs[0].device).cuda_stream
+    _check(lib().sal_solve_joint(gh, k, sp, nf, ld, xp, yp, ld, C.c_void_p(st)))
+    return outs
 
 
 def read_values(path, count) -> np.ndarray:

@@ -233,3 +233,32 @@ def test_autotune_picks_a_setting_within_the_bar():
     with pytest.raises(S.SalError):
         grid.autotune(ssh, ntargets=1000, max_rel_err=1e-12)
     assert grid.tune() == best        # a failed search leaves the setting as it was
+
+
+def test_joint_solve_of_uneven_grids_equals_separate_solves():
+    """sal_solve_joint runs the leaf passes of grids of different sizes in one
+    launch.  Each target group's work is the same wherever it runs, so every
+    result equals the grid's own sal_solve bit for bit."""
+    torch = _torch()
+    import salgpu as S
+    cases = [("small_3000", 20, 3), ("small_20000", 60, 64), ("cfg0", 100, 7)]
+    grids, sshs = [], []
+    for name, thresh, nf in cases:
+        S_, g, hs, grid = _grid(name, thresh, nf, seed=21)
+        grid2 = S.Grid(S.tree_traverse(g.xs, g.ys, g.zs, g.n, thresh), g.xs, g.ys, g.zs, g.areas, 8, S.MODE_DTT,
+                       S.dual_tree_traversal(S.tree_traverse(g.xs, g.ys, g.zs, g.n, thresh), 0.7, thresh),
+                       max_fields=64)
+        grids.append(grid2)
+        sshs.append(torch.tensor(hs, device="cuda"))
+    alone = [g.solve(s, form=S.FORM_MIXED) for g, s in zip(grids, sshs)]
+    joint = S.solve_joint(grids, sshs)
+    torch.cuda.synchronize()
+    for g in grids:
+        g.sync()
+    for (ax, ay), (jx, jy) in zip(alone, joint):
+        assert torch.equal(ax, jx) and torch.equal(ay, jy)
+    with pytest.raises(S.SalError):
+        S.solve_joint([grids[0], grids[0]], [sshs[0], sshs[0]])
+    g9 = _grid("small_3000", 20, 3, seed=21, degree=9)[3]
+    with pytest.raises(S.SalError):
+        S.solve_joint([grids[0], g9], [sshs[0], sshs[0]])
