@@ -83,7 +83,7 @@ struct GridImpl {
     double *tgt_nodes = nullptr;
     // tcgen05 plan (tree passes, its own proxy units)
     int32_t *m2m_tasks = nullptr, *l2l_tasks = nullptr, *tc_proxy_unit_beg = nullptr;
-    double *tc_up_nodes = nullptr, *tc_down_nodes = nullptr;
+    double *tc_up_nodes = nullptr, *tc_down_nodes = nullptr, *tc_transfer = nullptr;
     int64_t mix_bytes = 0;
     std::vector<std::pair<void **, size_t>> mix_allocs;   // the batched form's buffers (release_mixed frees them)
     // staging for the *_host entry points
@@ -504,6 +504,7 @@ static int ensure_mixed(GridImpl &g, int FT) {
         if (!rc) rc = upload_mix(g, &g.tc_down_nodes, pl.tc_down_nodes);
         if (!rc) rc = upload_mix(g, &g.m2m_tasks, pl.m2m_tasks);
         if (!rc) rc = upload_mix(g, &g.l2l_tasks, pl.l2l_tasks);
+        if (!rc) rc = upload_mix(g, &g.tc_transfer, pl.tc_transfer);
         const int64_t nbk = (int64_t)pl.tc_bas.size() / 3,
                       nunits = pl.tc_up_unit_beg.empty() ? 0 : pl.tc_up_unit_beg.back();
         if (!rc) rc = malloc_mix(g, &g.tc_up_partial, (size_t)nunits * P * FT);
@@ -635,8 +636,8 @@ static void solve_mixed_block(GridImpl &g, const double *ssh, int64_t ld_ssh, in
         }
         if (tree)
             for (size_t l = 0; l + 1 < pl.m2m_level_beg.size(); ++l)
-                mix::launch_m2m(g.m2m_tasks + 5 * (size_t)pl.m2m_level_beg[l], pl.m2m_level_beg[l + 1] - pl.m2m_level_beg[l],
-                                g.tc_up_nodes, pl.d + 1, g.wF + (size_t)n * FT, st);
+                mix::launch_m2m(g.m2m_tasks + 6 * (size_t)pl.m2m_level_beg[l], pl.m2m_level_beg[l + 1] - pl.m2m_level_beg[l],
+                                g.tc_transfer, pl.d + 1, g.wF + (size_t)n * FT, st);
         mix::launch_split_store(g.bsrc, pl.tc_pt_ksteps, pl.tc_src_ksteps, g.wF, g.phiF, g.bstore, st);
     } else if (!pl.mix_up_groups.empty()) {
         mix::MixArgs u = a;
@@ -663,8 +664,8 @@ static void solve_mixed_block(GridImpl &g, const double *ssh, int64_t ld_ssh, in
         mix::launch_finalize_mix(g.tc_proxy_unit_beg, g.mix_proxy_partial, g.ntgt, 3 * P, FT, g.phiF, st);
         if (tree)
             for (size_t l = 0; l + 1 < pl.l2l_level_beg.size(); ++l)
-                mix::launch_l2l(g.l2l_tasks + 3 * (size_t)pl.l2l_level_beg[l], pl.l2l_level_beg[l + 1] - pl.l2l_level_beg[l],
-                                g.tc_down_nodes, pl.d + 1, g.phiF, st);
+                mix::launch_l2l(g.l2l_tasks + 4 * (size_t)pl.l2l_level_beg[l], pl.l2l_level_beg[l + 1] - pl.l2l_level_beg[l],
+                                g.tc_transfer, pl.d + 1, g.phiF, st);
     } else if (!pl.mix_proxy_groups.empty()) {
         mix::MixArgs q = a;
         q.groups = g.mix_proxy_groups;

@@ -89,9 +89,10 @@ void launch_source_local(const double4 *pool, const int2 *ranges, const double4 
                          cudaStream_t st);
 void launch_self_pair(const double4 *pool, int n, double2 *selfk, cudaStream_t st);
 void launch_source_ksteps(const int32_t *bsrc, int64_t nks, const float4 *sloc, float *sxyz, cudaStream_t st);
-// tree transfers (transfer.cu): one launch per tree level
-void launch_m2m(const int32_t *tasks, int ntasks, const double *nodes, int n, float *w, cudaStream_t st);
-void launch_l2l(const int32_t *tasks, int ntasks, const double *nodes, int n, float *phi, cudaStream_t st);
+// tree transfers (transfer.cu): one launch per tree level; H holds the two
+// n x n half-interval transfer matrices
+void launch_m2m(const int32_t *tasks, int ntasks, const double *H, int n, float *w, cudaStream_t st);
+void launch_l2l(const int32_t *tasks, int ntasks, const double *H, int n, float *phi, cudaStream_t st);
 
 }  // namespace mix
 }  // namespace sal

@@ -48,6 +48,27 @@ static void panel_proxies(const Panel &q, int d, double *xyz, double *nodes, dou
     if (box) { box[0] = q.min_xi; box[1] = q.max_xi; box[2] = q.min_eta; box[3] = q.max_eta; }
 }
 
+// interp_vals_bli's one-dimensional basis (bli_module.f90:67-105): the
+// exact-node test, then the second barycentric form normalised by its
+// denominator; weights 1/2, -1, 1, ..., (-1)^d / 2 (bli_module.f90:13-24).
+void bli_basis_host(double x, const double *nodes, int n, double *f) {
+    bool found = false;
+    for (int i = 0; i < n; ++i) {
+        f[i] = 0.0;
+        if (std::fabs(x - nodes[i]) < 1e-16) { found = true; f[i] = 1.0; }
+    }
+    if (found) return;
+    double denom = 0.0;
+    for (int i = 0; i < n; ++i) {
+        double c = (i & 1) ? -1.0 : 1.0;
+        if (n == 1) c = 1.0;
+        else if (i == 0 || i == n - 1) c *= 0.5;
+        f[i] = c / (x - nodes[i]);
+        denom += f[i];
+    }
+    for (int i = 0; i < n; ++i) f[i] /= denom;
+}
+
 static void push_range(std::vector<Item> &v, int64_t off, int64_t cnt, int kind, int32_t mask) {
     for (int64_t b = 0; b < cnt; b += kMaxStage) {
         int64_t c = std::min<int64_t>(kMaxStage, cnt - b);
@@ -440,28 +461,54 @@ bool plan_build_tc(const Tree &t, Plan *pl, const TcOptions &opt, std::string *e
             if (wslot[k] >= 0 && !q.is_leaf && q.count() > 0) up[q.level].push_back(k);
             if (dslot[k] >= 0 && q.parent >= 1 && dslot[q.parent - 1] >= 0) down[q.level].push_back(k);
         }
+        // which half of its parent's xi (bit 0) and eta (bit 1) interval a
+        // child covers: 0 the lower half, 1 the upper
+        auto halves = [&](int ch) {
+            const Panel &c = t.p[ch], &q = t.p[c.parent - 1];
+            return (c.min_xi < q.mid_xi ? 0 : 1) | (c.min_eta < q.mid_eta ? 0 : 2);
+        };
         for (int l = maxl; l >= 0; --l) {
             if (up[l].empty()) continue;
-            pl->m2m_level_beg.push_back((int32_t)(pl->m2m_tasks.size() / 5));
+            pl->m2m_level_beg.push_back((int32_t)(pl->m2m_tasks.size() / 6));
             for (int k : up[l]) {
                 pl->m2m_tasks.push_back(wslot[k]);
+                int32_t code = 0;
                 for (int c = 0; c < 4; ++c) {
                     const int ch = t.p[k].child[c];
-                    pl->m2m_tasks.push_back(ch >= 1 && t.p[ch - 1].count() > 0 ? wslot[ch - 1] : -1);
+                    const bool live = ch >= 1 && t.p[ch - 1].count() > 0;
+                    pl->m2m_tasks.push_back(live ? wslot[ch - 1] : -1);
+                    if (live) code |= halves(ch - 1) << (2 * c);
                 }
+                pl->m2m_tasks.push_back(code);
             }
         }
-        pl->m2m_level_beg.push_back((int32_t)(pl->m2m_tasks.size() / 5));
+        pl->m2m_level_beg.push_back((int32_t)(pl->m2m_tasks.size() / 6));
         for (int l = 0; l <= maxl; ++l) {
             if (down[l].empty()) continue;
-            pl->l2l_level_beg.push_back((int32_t)(pl->l2l_tasks.size() / 3));
+            pl->l2l_level_beg.push_back((int32_t)(pl->l2l_tasks.size() / 4));
             for (int k : down[l]) {
                 pl->l2l_tasks.push_back(dslot[k]);
                 pl->l2l_tasks.push_back(dslot[t.p[k].parent - 1]);
                 pl->l2l_tasks.push_back(tgt_slot[k] >= 0 ? 1 : 0);
+                pl->l2l_tasks.push_back(halves(k));
             }
         }
-        pl->l2l_level_beg.push_back((int32_t)(pl->l2l_tasks.size() / 3));
+        pl->l2l_level_beg.push_back((int32_t)(pl->l2l_tasks.size() / 4));
+        // The transfer matrices.  Barycentric Lagrange bases are invariant
+        // under affine maps of the interval, so one pair serves every panel:
+        // H[h][j][i] = the parent's basis j (nodes on [-1, 1]) at node i of
+        // its lower (h = 0, [-1, 0]) or upper (h = 1, [0, 1]) half.
+        pl->tc_transfer.assign(2 * (size_t)nd * nd, 0.0);
+        double pn[kMaxDegree + 1], cn[kMaxDegree + 1];
+        cheb_nodes(-1.0, 1.0, d, pn);
+        for (int h = 0; h < 2; ++h) {
+            cheb_nodes(h ? 0.0 : -1.0, h ? 1.0 : 0.0, d, cn);
+            for (int i = 0; i < nd; ++i) {
+                double f[kMaxDegree + 1];
+                bli_basis_host(cn[i], pn, nd, f);
+                for (int j = 0; j < nd; ++j) pl->tc_transfer[((size_t)h * nd + j) * nd + i] = f[j];
+            }
+        }
     }
 
     // ---- the split weight store's row map

@@ -40,6 +40,7 @@ void face_xieta(double x, double y, double z, int face, double *xi, double *eta)
 void xyz_from_xieta(double xi, double eta, int face, double *x, double *y, double *z);
 int face_from_xyz(double x, double y, double z);
 void cheb_nodes(double min_x, double max_x, int degree, double *out);
+void bli_basis_host(double x, const double *nodes, int n, double *f);
 
 Tree *tree_build(const double *xs, const double *ys, const double *zs, int32_t n, int32_t thresh);
 Tree *tree_import(int32_t npanels, const int32_t *ints9, const double *dbl7, const int64_t *pt_off,
@@ -173,10 +174,13 @@ struct Plan {
     TcOptions tc_opt;
     int32_t n_wslots = 0, n_dslots = 0;
     std::vector<double> tc_up_nodes, tc_down_nodes;
-    std::vector<int32_t> m2m_tasks;               // per refined up panel: parent wslot, 4 child wslots (-1: none)
+    std::vector<int32_t> m2m_tasks;               // per refined up panel: parent wslot, 4 child wslots (-1: none),
+                                                  // the children's halves (2 bits each: xi, eta upper)
     std::vector<int32_t> m2m_level_beg;           // task ranges per level, deepest first
-    std::vector<int32_t> l2l_tasks;               // per down panel under another: child dslot, parent dslot, own
+    std::vector<int32_t> l2l_tasks;               // per down panel under another: child dslot, parent dslot, own,
+                                                  // the child's halves
     std::vector<int32_t> l2l_level_beg;           // task ranges per level, top first
+    std::vector<double> tc_transfer;              // [half][j][i]: parent basis j at node i of its lower / upper half
     double tc_macs_up = 0, tc_macs_down = 0;      // per field: basis MACs of the batched form's upward / DOWN work
     double pairs[4] = {0, 0, 0, 0};               // PP, PC, CP, CC evaluations per field
     double macs_up = 0, macs_down = 0;

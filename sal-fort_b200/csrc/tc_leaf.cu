@@ -31,7 +31,8 @@
 //   warp 9      loads, per stage, the weight tiles (pre-split TF32 hi / lo,
 //               written once per solve by split_store_kernel) and the
 //               sources' coordinates (leaf and proxy passes) or BLI factors
-//               (upward pass), with bulk copies into a 3-deep ring.
+//               (upward pass), with bulk copies into a 4-deep ring, and
+//               prefetches the next item's tiles into L2.
 //   warps 10-13 fold finished accumulator chains into the running sums and
 //               write the outputs (warp w: tensor memory lanes 32(w%4)..+31).
 // The tensor cores accumulate with truncation, so one chain over all of a
@@ -64,7 +65,7 @@ constexpr int kF = 64;                            // fields
 constexpr int kStageK = 32;                       // K columns per stage (four k-steps of 8)
 constexpr int kStageKs = kStageK / 8;             // k-steps per stage
 constexpr int kKStages = 2;                       // kernel-tile ring
-constexpr int kWStages = 3;                       // weight / upward-factor ring
+constexpr int kWStages = 4;                       // weight / upward-factor ring
 constexpr int kAuxFloats = kStageKs * 16 * (kMaxDegree + 1);   // upward factors of a stage's k-steps
 constexpr int kTileFloats = 2048;                 // kernel tile of one k-step: 256 rows x 8, one of hi / lo
 constexpr int kWStepFloats = 1024;                // weight tile of one k-step: 128 rows x 8
@@ -117,6 +118,12 @@ __device__ __forceinline__ float tf32_hi(float x) {
     uint32_t r;
     asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
     return __uint_as_float(r);
+}
+
+// Hint: fetch a global range into L2 ahead of its bulk copy (16-byte
+// aligned, a multiple of 16 bytes).
+__device__ __forceinline__ void prefetch_l2(const void *p, uint32_t bytes) {
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
 }
 
 __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
@@ -659,7 +666,16 @@ __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(const __grid_const
             TcItem nxt = G.ib < G.ie ? a.items[G.ib] : TcItem{};
             for (int k = G.ib; k < G.ie; ++k) {
                 const TcItem it = nxt;
-                if (k + 1 < G.ie) nxt = a.items[k + 1];
+                if (k + 1 < G.ie) {
+                    nxt = a.items[k + 1];
+                    // the next item's weight tiles (and source coordinates)
+                    // into L2 while this item's stages run
+                    if (lane == 0 && MODE != 2) {
+                        const uint32_t nks = (uint32_t)(nxt.cnt + 7) >> 3;
+                        prefetch_l2(a.bstore + (size_t)nxt.kb * kWStepFloats, nks * kWStepFloats * 4u);
+                        if ((nxt.kind & 3) != 2) prefetch_l2(a.sxyz + (size_t)nxt.kb * 24, nks * 96u);
+                    }
+                }
                 const int nst = (it.cnt + kStageK - 1) / kStageK;
                 for (int j = 0; j < nst; ++j, ++st) {
                     const uint32_t jb = st % kWStages, ub = st / kWStages;
@@ -822,6 +838,8 @@ __global__ void self_pair_kernel(const double4 *__restrict__ pool, int n, double
     if (T.live) dev::gref_exact(T, c.x, c.y, c.z, sx, sy);
     selfk[p] = make_double2(sx / dev::kCons, sy / dev::kCons);
 }
+
+static_assert(sizeof(TcSmem) + 1024 <= 227 * 1024, "the leaf kernel's shared memory fits one SM");
 
 size_t tc_smem_bytes() {
     // above half of the SM's shared memory: one CTA per SM, which owns all
