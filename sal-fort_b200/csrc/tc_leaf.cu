@@ -313,7 +313,7 @@ __device__ __noinline__ void fold_chain(uint32_t td, int q, int lane, bool end, 
 // gi belongs to the grid k with J.beg[k] <= gi < J.beg[k + 1] and carries
 // that grid's arguments.  Otherwise J.g[0] is the only grid.
 template <int MODE, bool JOINT>
-__global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(const __grid_constant__ TcJoint J, int *err) {
+__global__ void __maxnreg__(128) tc_leaf_kernel(const __grid_constant__ TcJoint J, int *err) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     TcSmem &sm = *reinterpret_cast<TcSmem *>(smem_raw);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -476,122 +476,148 @@ __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(const __grid_const
                     if ((MODE == 2 || kind != 2) && active && kfirst < nks)
                         wait_bounded(&sm.wfull[st % kWStages], (st / kWStages) & 1, abort, err);
                     const float4 *crd = reinterpret_cast<const float4 *>(sm.aux[st % kWStages]);
+                    // one task: the kernel-tile values of k-step kk for this
+                    // lane's row (east / north, or the three Cartesian
+                    // components in the proxy pass)
+                    auto values = [&](int kk, float (&ve)[8], float (&vn)[8], float (&vz)[8]) {
+                            if (MODE == 2) {
+                                // upward: the BLI basis of proxy (i, j) at the 8 points,
+                                // F_i(xi) G_j(eta) from the per-point factors
+                                const float *Fb = sm.aux[st % kWStages] + 16 * n * kk;
+                                const float4 f0 = *reinterpret_cast<const float4 *>(Fb + 8 * up_i);
+                                const float4 f1 = *reinterpret_cast<const float4 *>(Fb + 8 * up_i + 4);
+                                const float4 g0 = *reinterpret_cast<const float4 *>(Fb + 8 * n + 8 * up_j);
+                                const float4 g1 = *reinterpret_cast<const float4 *>(Fb + 8 * n + 8 * up_j + 4);
+                                ve[0] = f0.x * g0.x; ve[1] = f0.y * g0.y; ve[2] = f0.z * g0.z; ve[3] = f0.w * g0.w;
+                                ve[4] = f1.x * g1.x; ve[5] = f1.y * g1.y; ve[6] = f1.z * g1.z; ve[7] = f1.w * g1.w;
+    #pragma unroll
+                                for (int c = 0; c < 8; ++c) vn[c] = 0.f;
+                            } else if (MODE == 0 && kind == 2) {
+                                // DOWN: BLI basis of the target x its unit vector's
+                                // component of the Cartesian row
+                                const int *km0 = sm.kmap + it.row0 + kStageK * j + 8 * kk;
+                                const float *fxr = sm.fx[row], *fer = sm.fe[row];
+    #pragma unroll
+                                for (int c = 0; c < 8; ++c) {
+                                    const int km = km0[c];
+                                    const float b = fxr[km & 255] * fer[(km >> 8) & 255];
+                                    const int comp = km >> 16;
+                                    ve[c] = comp == 2 ? 0.f : b * (comp == 0 ? el0 : el1);
+                                    vn[c] = b * (comp == 0 ? ep0 : (comp == 1 ? ep1 : ep2));
+                                }
+                            } else {
+                                // PP / PC: kernel value x projected displacement,
+                                // two columns per packed instruction
+                                // this k-step's x[8] y[8] z[8] (same address in every
+                                // lane: shared-memory broadcasts)
+                                float4 pre[6];
+    #pragma unroll
+                                for (int i = 0; i < 6; ++i) pre[i] = crd[6 * kk + i];
+    #pragma unroll
+                                for (int c2 = 0; c2 < 4; ++c2) {
+                                    // pre[0..1] = x[8], pre[2..3] = y[8], pre[4..5] = z[8]
+                                    const float4 X = pre[c2 >> 1], Y = pre[2 + (c2 >> 1)], Z = pre[4 + (c2 >> 1)];
+                                    const float2 dx = sub2((c2 & 1) ? make_float2(X.z, X.w) : make_float2(X.x, X.y), tx2);
+                                    const float2 dy = sub2((c2 & 1) ? make_float2(Y.z, Y.w) : make_float2(Y.x, Y.y), ty2);
+                                    const float2 dz = sub2((c2 & 1) ? make_float2(Z.z, Z.w) : make_float2(Z.x, Z.y), tz2);
+                                    float2 mp = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
+                                    // mp = 0 only for a source on the target itself (or a
+                                    // repeated point): the clamp keeps the value finite
+                                    mp.x = fmaxf(mp.x, 1e-20f);
+                                    mp.y = fmaxf(mp.y, 1e-20f);
+                                    const float2 r = make_float2(rsqrt_approx(mp.x), rsqrt_approx(mp.y));
+                                    const float2 w = __fadd2_rn(__fmul2_rn(mp, r), f2(2.f));
+                                    const float2 u = make_float2(rcp_approx(w.x), rcp_approx(w.y));
+                                    const float2 inner = __ffma2_rn(f2(kC1F), r, __ffma2_rn(f2(kTwoC2F), u, f2(-kTwoC2F)));
+                                    const float2 v = __fmul2_rn(inner, __fmul2_rn(r, r));
+                                    if (MODE == 0) {
+                                        const float2 pe = __ffma2_rn(el1v, dy, __fmul2_rn(el0v, dx));
+                                        const float2 pn = __ffma2_rn(ep2v, dz, __ffma2_rn(ep1v, dy, __fmul2_rn(ep0v, dx)));
+                                        const float2 e2 = __fmul2_rn(v, pe), n2 = __fmul2_rn(v, pn);
+                                        ve[2 * c2] = e2.x;
+                                        ve[2 * c2 + 1] = e2.y;
+                                        vn[2 * c2] = n2.x;
+                                        vn[2 * c2 + 1] = n2.y;
+                                    } else {
+                                        // proxy targets: the Cartesian vector val (s - x)
+                                        const float2 x2 = __fmul2_rn(v, dx), y2 = __fmul2_rn(v, dy), z2 = __fmul2_rn(v, dz);
+                                        ve[2 * c2] = x2.x;
+                                        ve[2 * c2 + 1] = x2.y;
+                                        vn[2 * c2] = y2.x;
+                                        vn[2 * c2 + 1] = y2.y;
+                                        vz[2 * c2] = z2.x;
+                                        vz[2 * c2 + 1] = z2.y;
+                                    }
+                                }
+                                // the target itself among these 8 sources: the self pair
+                                if (self_item) {
+                                    const int cs = my_pos - (it.off + kStageK * j + 8 * kk);
+                                    if ((unsigned)cs < 8u) {
+    #pragma unroll
+                                        for (int c = 0; c < 8; ++c)
+                                            if (c == cs) { ve[c] = self_e; vn[c] = self_n; }
+                                    }
+                                }
+                            }
+                    };
+                    // its TF32 hi + lo split, stored into the kernel tile
+                    auto store = [&](int kk, const float (&ve)[8], const float (&vn)[8], const float (&vz)[8]) {
+                            // TF32 hi + lo (the tensor cores read lo's top 11 bits)
+                            float *th = sm.Kt[slot][kk][0], *tlo = sm.Kt[slot][kk][1];
+    #pragma unroll
+                            for (int hh = 0; hh < 2; ++hh) {
+                                const float4 eh = make_float4(tf32_hi(ve[4 * hh]), tf32_hi(ve[4 * hh + 1]),
+                                                              tf32_hi(ve[4 * hh + 2]), tf32_hi(ve[4 * hh + 3]));
+                                const float4 nh = make_float4(tf32_hi(vn[4 * hh]), tf32_hi(vn[4 * hh + 1]),
+                                                              tf32_hi(vn[4 * hh + 2]), tf32_hi(vn[4 * hh + 3]));
+                                const float2 el01 = sub2(make_float2(ve[4 * hh], ve[4 * hh + 1]), make_float2(eh.x, eh.y));
+                                const float2 el23 = sub2(make_float2(ve[4 * hh + 2], ve[4 * hh + 3]), make_float2(eh.z, eh.w));
+                                const float2 nl01 = sub2(make_float2(vn[4 * hh], vn[4 * hh + 1]), make_float2(nh.x, nh.y));
+                                const float2 nl23 = sub2(make_float2(vn[4 * hh + 2], vn[4 * hh + 3]), make_float2(nh.z, nh.w));
+                                if (row_in_tile) {
+                                    *reinterpret_cast<float4 *>(th + oe + 32 * hh) = eh;
+                                    *reinterpret_cast<float4 *>(tlo + oe + 32 * hh) = make_float4(el01.x, el01.y, el23.x, el23.y);
+                                    if (MODE != 2) {
+                                        *reinterpret_cast<float4 *>(th + on + 32 * hh) = nh;
+                                        *reinterpret_cast<float4 *>(tlo + on + 32 * hh) = make_float4(nl01.x, nl01.y, nl23.x, nl23.y);
+                                    }
+                                }
+                                if (MODE == 1) {
+                                    const float4 zh = make_float4(tf32_hi(vz[4 * hh]), tf32_hi(vz[4 * hh + 1]),
+                                                                  tf32_hi(vz[4 * hh + 2]), tf32_hi(vz[4 * hh + 3]));
+                                    const float2 zl01 = sub2(make_float2(vz[4 * hh], vz[4 * hh + 1]), make_float2(zh.x, zh.y));
+                                    const float2 zl23 = sub2(make_float2(vz[4 * hh + 2], vz[4 * hh + 3]), make_float2(zh.z, zh.w));
+                                    if (row_in_tile) {
+                                        *reinterpret_cast<float4 *>(th + oz + 32 * hh) = zh;
+                                        *reinterpret_cast<float4 *>(tlo + oz + 32 * hh) = make_float4(zl01.x, zl01.y, zl23.x, zl23.y);
+                                    }
+                                }
+                            }
+                    };
+                    // Full groups deal a warp two k-steps of one row block per
+                    // stage: computing both before storing either interleaves
+                    // their independent dependency chains.
 #pragma unroll 1
                     for (int kk = kfirst; active && kk < nks; kk += kstride) {
                         float ve[8], vn[8], vz[8];
-                        if (MODE == 2) {
-                            // upward: the BLI basis of proxy (i, j) at the 8 points,
-                            // F_i(xi) G_j(eta) from the per-point factors
-                            const float *Fb = sm.aux[st % kWStages] + 16 * n * kk;
-                            const float4 f0 = *reinterpret_cast<const float4 *>(Fb + 8 * up_i);
-                            const float4 f1 = *reinterpret_cast<const float4 *>(Fb + 8 * up_i + 4);
-                            const float4 g0 = *reinterpret_cast<const float4 *>(Fb + 8 * n + 8 * up_j);
-                            const float4 g1 = *reinterpret_cast<const float4 *>(Fb + 8 * n + 8 * up_j + 4);
-                            ve[0] = f0.x * g0.x; ve[1] = f0.y * g0.y; ve[2] = f0.z * g0.z; ve[3] = f0.w * g0.w;
-                            ve[4] = f1.x * g1.x; ve[5] = f1.y * g1.y; ve[6] = f1.z * g1.z; ve[7] = f1.w * g1.w;
-#pragma unroll
-                            for (int c = 0; c < 8; ++c) vn[c] = 0.f;
-                        } else if (MODE == 0 && kind == 2) {
-                            // DOWN: BLI basis of the target x its unit vector's
-                            // component of the Cartesian row
-                            const int *km0 = sm.kmap + it.row0 + kStageK * j + 8 * kk;
-                            const float *fxr = sm.fx[row], *fer = sm.fe[row];
-#pragma unroll
-                            for (int c = 0; c < 8; ++c) {
-                                const int km = km0[c];
-                                const float b = fxr[km & 255] * fer[(km >> 8) & 255];
-                                const int comp = km >> 16;
-                                ve[c] = comp == 2 ? 0.f : b * (comp == 0 ? el0 : el1);
-                                vn[c] = b * (comp == 0 ? ep0 : (comp == 1 ? ep1 : ep2));
+                        if (MODE != 2 && kstride == 2 && kk + 2 < nks) {
+                            float ve2[8], vn2[8], vz2[8];
+                            values(kk, ve, vn, vz);
+                            values(kk + 2, ve2, vn2, vz2);
+                            if (!slot_free) {
+                                wait_bounded(&sm.kempty[slot], kpar, abort, err);
+                                slot_free = true;
                             }
+                            store(kk, ve, vn, vz);
+                            store(kk + 2, ve2, vn2, vz2);
+                            kk += 2;
                         } else {
-                            // PP / PC: kernel value x projected displacement,
-                            // two columns per packed instruction
-                            // this k-step's x[8] y[8] z[8] (same address in every
-                            // lane: shared-memory broadcasts)
-                            float4 pre[6];
-#pragma unroll
-                            for (int i = 0; i < 6; ++i) pre[i] = crd[6 * kk + i];
-#pragma unroll
-                            for (int c2 = 0; c2 < 4; ++c2) {
-                                // pre[0..1] = x[8], pre[2..3] = y[8], pre[4..5] = z[8]
-                                const float4 X = pre[c2 >> 1], Y = pre[2 + (c2 >> 1)], Z = pre[4 + (c2 >> 1)];
-                                const float2 dx = sub2((c2 & 1) ? make_float2(X.z, X.w) : make_float2(X.x, X.y), tx2);
-                                const float2 dy = sub2((c2 & 1) ? make_float2(Y.z, Y.w) : make_float2(Y.x, Y.y), ty2);
-                                const float2 dz = sub2((c2 & 1) ? make_float2(Z.z, Z.w) : make_float2(Z.x, Z.y), tz2);
-                                float2 mp = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
-                                // mp = 0 only for a source on the target itself (or a
-                                // repeated point): the clamp keeps the value finite
-                                mp.x = fmaxf(mp.x, 1e-20f);
-                                mp.y = fmaxf(mp.y, 1e-20f);
-                                const float2 r = make_float2(rsqrt_approx(mp.x), rsqrt_approx(mp.y));
-                                const float2 w = __fadd2_rn(__fmul2_rn(mp, r), f2(2.f));
-                                const float2 u = make_float2(rcp_approx(w.x), rcp_approx(w.y));
-                                const float2 inner = __ffma2_rn(f2(kC1F), r, __ffma2_rn(f2(kTwoC2F), u, f2(-kTwoC2F)));
-                                const float2 v = __fmul2_rn(inner, __fmul2_rn(r, r));
-                                if (MODE == 0) {
-                                    const float2 pe = __ffma2_rn(el1v, dy, __fmul2_rn(el0v, dx));
-                                    const float2 pn = __ffma2_rn(ep2v, dz, __ffma2_rn(ep1v, dy, __fmul2_rn(ep0v, dx)));
-                                    const float2 e2 = __fmul2_rn(v, pe), n2 = __fmul2_rn(v, pn);
-                                    ve[2 * c2] = e2.x;
-                                    ve[2 * c2 + 1] = e2.y;
-                                    vn[2 * c2] = n2.x;
-                                    vn[2 * c2 + 1] = n2.y;
-                                } else {
-                                    // proxy targets: the Cartesian vector val (s - x)
-                                    const float2 x2 = __fmul2_rn(v, dx), y2 = __fmul2_rn(v, dy), z2 = __fmul2_rn(v, dz);
-                                    ve[2 * c2] = x2.x;
-                                    ve[2 * c2 + 1] = x2.y;
-                                    vn[2 * c2] = y2.x;
-                                    vn[2 * c2 + 1] = y2.y;
-                                    vz[2 * c2] = z2.x;
-                                    vz[2 * c2 + 1] = z2.y;
-                                }
+                            values(kk, ve, vn, vz);
+                            if (!slot_free) {
+                                wait_bounded(&sm.kempty[slot], kpar, abort, err);
+                                slot_free = true;
                             }
-                            // the target itself among these 8 sources: the self pair
-                            if (self_item) {
-                                const int cs = my_pos - (it.off + kStageK * j + 8 * kk);
-                                if ((unsigned)cs < 8u) {
-#pragma unroll
-                                    for (int c = 0; c < 8; ++c)
-                                        if (c == cs) { ve[c] = self_e; vn[c] = self_n; }
-                                }
-                            }
-                        }
-                        if (!slot_free) {
-                            wait_bounded(&sm.kempty[slot], kpar, abort, err);
-                            slot_free = true;
-                        }
-                        // TF32 hi + lo (the tensor cores read lo's top 11 bits)
-                        float *th = sm.Kt[slot][kk][0], *tlo = sm.Kt[slot][kk][1];
-#pragma unroll
-                        for (int hh = 0; hh < 2; ++hh) {
-                            const float4 eh = make_float4(tf32_hi(ve[4 * hh]), tf32_hi(ve[4 * hh + 1]),
-                                                          tf32_hi(ve[4 * hh + 2]), tf32_hi(ve[4 * hh + 3]));
-                            const float4 nh = make_float4(tf32_hi(vn[4 * hh]), tf32_hi(vn[4 * hh + 1]),
-                                                          tf32_hi(vn[4 * hh + 2]), tf32_hi(vn[4 * hh + 3]));
-                            const float2 el01 = sub2(make_float2(ve[4 * hh], ve[4 * hh + 1]), make_float2(eh.x, eh.y));
-                            const float2 el23 = sub2(make_float2(ve[4 * hh + 2], ve[4 * hh + 3]), make_float2(eh.z, eh.w));
-                            const float2 nl01 = sub2(make_float2(vn[4 * hh], vn[4 * hh + 1]), make_float2(nh.x, nh.y));
-                            const float2 nl23 = sub2(make_float2(vn[4 * hh + 2], vn[4 * hh + 3]), make_float2(nh.z, nh.w));
-                            if (row_in_tile) {
-                                *reinterpret_cast<float4 *>(th + oe + 32 * hh) = eh;
-                                *reinterpret_cast<float4 *>(tlo + oe + 32 * hh) = make_float4(el01.x, el01.y, el23.x, el23.y);
-                                if (MODE != 2) {
-                                    *reinterpret_cast<float4 *>(th + on + 32 * hh) = nh;
-                                    *reinterpret_cast<float4 *>(tlo + on + 32 * hh) = make_float4(nl01.x, nl01.y, nl23.x, nl23.y);
-                                }
-                            }
-                            if (MODE == 1) {
-                                const float4 zh = make_float4(tf32_hi(vz[4 * hh]), tf32_hi(vz[4 * hh + 1]),
-                                                              tf32_hi(vz[4 * hh + 2]), tf32_hi(vz[4 * hh + 3]));
-                                const float2 zl01 = sub2(make_float2(vz[4 * hh], vz[4 * hh + 1]), make_float2(zh.x, zh.y));
-                                const float2 zl23 = sub2(make_float2(vz[4 * hh + 2], vz[4 * hh + 3]), make_float2(zh.z, zh.w));
-                                if (row_in_tile) {
-                                    *reinterpret_cast<float4 *>(th + oz + 32 * hh) = zh;
-                                    *reinterpret_cast<float4 *>(tlo + oz + 32 * hh) = make_float4(zl01.x, zl01.y, zl23.x, zl23.y);
-                                }
-                            }
+                            store(kk, ve, vn, vz);
                         }
                     }
                     if (!slot_free) {
