@@ -287,6 +287,33 @@ __device__ __noinline__ void fold_chain(uint32_t td, int q, int lane, bool end, 
     const int per = (MODE != 1 && end) ? (nt + 15) / 16 : 8;
     const int nchunk = MODE == 2 ? per : 2 * per;   // upward: one component, columns 0..127
     auto col = [&](int i) { return (i / per) * 128 + (i % per) * 16; };
+    if (!end) {
+        // mid-group: the MMA warp waits for this fold before its next chain,
+        // so two chunks' loads are in flight per wait (nchunk is even here)
+        float x0[16], x1[16], r0[16], r1[16];
+#pragma unroll 1
+        for (int i = 0; i < nchunk; i += 2) {
+            const int c0 = col(i), c1 = col(i + 1);
+            tmem_ld16(td + c0, x0);
+            tmem_ld16(td + c1, x1);
+            if (!first) {
+                tmem_ld16(td + 256 + c0, r0);
+                tmem_ld16(td + 256 + c1, r1);
+            }
+            tmem_wait_ld();
+            if (!first) {
+#pragma unroll
+                for (int m = 0; m < 16; ++m) {
+                    x0[m] += r0[m];
+                    x1[m] += r1[m];
+                }
+            }
+            tmem_st16(td + 256 + c0, x0);
+            tmem_st16(td + 256 + c1, x1);
+        }
+        tmem_wait_st();
+        return;
+    }
     float x[16], r[16];
 #pragma unroll 1
     for (int i = 0; i < nchunk; ++i) {
@@ -298,15 +325,10 @@ __device__ __noinline__ void fold_chain(uint32_t td, int q, int lane, bool end, 
 #pragma unroll
             for (int m = 0; m < 16; ++m) x[m] += r[m];
         }
-        if (!end) {
-            tmem_st16(td + 256 + c, x);
-        } else {
-            const int ik = (c & 127) >> 5;
-            const int idk = ik == 0 ? idx[0] : ik == 1 ? idx[1] : ik == 2 ? idx[2] : idx[3];
-            emit_chunk<MODE>(x, c, f, odd, nt, idk, c < 128 ? ox : oy, wr, part);
-        }
+        const int ik = (c & 127) >> 5;
+        const int idk = ik == 0 ? idx[0] : ik == 1 ? idx[1] : ik == 2 ? idx[2] : idx[3];
+        emit_chunk<MODE>(x, c, f, odd, nt, idk, c < 128 ? ox : oy, wr, part);
     }
-    if (!end) tmem_wait_st();
 }
 
 // JOINT: one launch over the groups of several grids (of one degree): group
@@ -490,14 +512,14 @@ __global__ void __maxnreg__(128) tc_leaf_kernel(const __grid_constant__ TcJoint 
                                 const float4 g1 = *reinterpret_cast<const float4 *>(Fb + 8 * n + 8 * up_j + 4);
                                 ve[0] = f0.x * g0.x; ve[1] = f0.y * g0.y; ve[2] = f0.z * g0.z; ve[3] = f0.w * g0.w;
                                 ve[4] = f1.x * g1.x; ve[5] = f1.y * g1.y; ve[6] = f1.z * g1.z; ve[7] = f1.w * g1.w;
-    #pragma unroll
+#pragma unroll
                                 for (int c = 0; c < 8; ++c) vn[c] = 0.f;
                             } else if (MODE == 0 && kind == 2) {
                                 // DOWN: BLI basis of the target x its unit vector's
                                 // component of the Cartesian row
                                 const int *km0 = sm.kmap + it.row0 + kStageK * j + 8 * kk;
                                 const float *fxr = sm.fx[row], *fer = sm.fe[row];
-    #pragma unroll
+#pragma unroll
                                 for (int c = 0; c < 8; ++c) {
                                     const int km = km0[c];
                                     const float b = fxr[km & 255] * fer[(km >> 8) & 255];
@@ -511,9 +533,9 @@ __global__ void __maxnreg__(128) tc_leaf_kernel(const __grid_constant__ TcJoint 
                                 // this k-step's x[8] y[8] z[8] (same address in every
                                 // lane: shared-memory broadcasts)
                                 float4 pre[6];
-    #pragma unroll
+#pragma unroll
                                 for (int i = 0; i < 6; ++i) pre[i] = crd[6 * kk + i];
-    #pragma unroll
+#pragma unroll
                                 for (int c2 = 0; c2 < 4; ++c2) {
                                     // pre[0..1] = x[8], pre[2..3] = y[8], pre[4..5] = z[8]
                                     const float4 X = pre[c2 >> 1], Y = pre[2 + (c2 >> 1)], Z = pre[4 + (c2 >> 1)];
@@ -553,7 +575,7 @@ __global__ void __maxnreg__(128) tc_leaf_kernel(const __grid_constant__ TcJoint 
                                 if (self_item) {
                                     const int cs = my_pos - (it.off + kStageK * j + 8 * kk);
                                     if ((unsigned)cs < 8u) {
-    #pragma unroll
+#pragma unroll
                                         for (int c = 0; c < 8; ++c)
                                             if (c == cs) { ve[c] = self_e; vn[c] = self_n; }
                                     }
@@ -564,7 +586,7 @@ __global__ void __maxnreg__(128) tc_leaf_kernel(const __grid_constant__ TcJoint 
                     auto store = [&](int kk, const float (&ve)[8], const float (&vn)[8], const float (&vz)[8]) {
                             // TF32 hi + lo (the tensor cores read lo's top 11 bits)
                             float *th = sm.Kt[slot][kk][0], *tlo = sm.Kt[slot][kk][1];
-    #pragma unroll
+#pragma unroll
                             for (int hh = 0; hh < 2; ++hh) {
                                 const float4 eh = make_float4(tf32_hi(ve[4 * hh]), tf32_hi(ve[4 * hh + 1]),
                                                               tf32_hi(ve[4 * hh + 2]), tf32_hi(ve[4 * hh + 3]));
