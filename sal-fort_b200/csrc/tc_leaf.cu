@@ -335,7 +335,7 @@ __device__ __noinline__ void fold_chain(uint32_t td, int q, int lane, bool end, 
 // gi belongs to the grid k with J.beg[k] <= gi < J.beg[k + 1] and carries
 // that grid's arguments.  Otherwise J.g[0] is the only grid.
 template <int MODE, bool JOINT>
-__global__ void __maxnreg__(128) tc_leaf_kernel(const __grid_constant__ TcJoint J, int *err) {
+__global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(const __grid_constant__ TcJoint J, int *err) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     TcSmem &sm = *reinterpret_cast<TcSmem *>(smem_raw);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -616,31 +616,15 @@ __global__ void __maxnreg__(128) tc_leaf_kernel(const __grid_constant__ TcJoint 
                                 }
                             }
                     };
-                    // Full groups deal a warp two k-steps of one row block per
-                    // stage: computing both before storing either interleaves
-                    // their independent dependency chains.
 #pragma unroll 1
                     for (int kk = kfirst; active && kk < nks; kk += kstride) {
                         float ve[8], vn[8], vz[8];
-                        if (MODE != 2 && kstride == 2 && kk + 2 < nks) {
-                            float ve2[8], vn2[8], vz2[8];
-                            values(kk, ve, vn, vz);
-                            values(kk + 2, ve2, vn2, vz2);
-                            if (!slot_free) {
-                                wait_bounded(&sm.kempty[slot], kpar, abort, err);
-                                slot_free = true;
-                            }
-                            store(kk, ve, vn, vz);
-                            store(kk + 2, ve2, vn2, vz2);
-                            kk += 2;
-                        } else {
-                            values(kk, ve, vn, vz);
-                            if (!slot_free) {
-                                wait_bounded(&sm.kempty[slot], kpar, abort, err);
-                                slot_free = true;
-                            }
-                            store(kk, ve, vn, vz);
+                        values(kk, ve, vn, vz);
+                        if (!slot_free) {
+                            wait_bounded(&sm.kempty[slot], kpar, abort, err);
+                            slot_free = true;
                         }
+                        store(kk, ve, vn, vz);
                     }
                     if (!slot_free) {
                         // warps that wrote nothing: their arrival must still
