@@ -56,6 +56,8 @@ def _args():
     ap.add_argument("--serve-host", action="store_true", help="serving requests carry host arrays")
     ap.add_argument("--no-serve", action="store_true")
     ap.add_argument("--no-autotune", action="store_true", help="time the batched form's default settings")
+    ap.add_argument("--tune", default=None,
+                    help="batched form's settings as name=value,... (sal_tune fields); replaces the autotuner")
     ap.add_argument("--no-stt", action="store_true", help="skip the mom6_code.f90 path measurement")
     ap.add_argument("--cpu-table", action="store_true", help="time the oracle on cfg0/cfg1/cfg2 and exit")
     a = ap.parse_args()
@@ -498,6 +500,17 @@ def main():
     tree = S.tree_traverse(g.xs, g.ys, g.zs, g.n, args.thresh)
     inter = S.dual_tree_traversal(tree, args.theta, args.thresh)
     t_lists = time.perf_counter() - t0
+    # the same tree and list built on the device (fast admission); the host
+    # build above stays the one solved
+    # (the first device build at this size loads its kernels: time the second)
+    S.dual_tree_traversal(S.tree_traverse(g.xs, g.ys, g.zs, g.n, args.thresh, device=local),
+                          args.theta, args.thresh, device=local)
+    t0 = time.perf_counter()
+    dtree = S.tree_traverse(g.xs, g.ys, g.zs, g.n, args.thresh, device=local)
+    dinter = S.dual_tree_traversal(dtree, args.theta, args.thresh, device=local)
+    t_lists_dev = time.perf_counter() - t0
+    dev_build_same = bool(np.array_equal(dinter, inter))
+    del dtree, dinter
     grid = S.Grid(tree, g.xs, g.ys, g.zs, g.areas, args.degree, S.MODE_DTT, inter, device=local, max_fields=F)
     st = grid.stats()
     ssh = torch.tensor(h, device=dev)                      # (F, N), resident before timing
@@ -507,7 +520,9 @@ def main():
     stream = torch.cuda.current_stream(dev)
 
     tuned = None
-    if form == S.FORM_MIXED and not args.no_autotune:
+    if form == S.FORM_MIXED and args.tune:
+        tuned = {"set": grid.tune(**{k: int(v) for k, v in (kv.split("=") for kv in args.tune.split(","))})}
+    elif form == S.FORM_MIXED and not args.no_autotune:
         # the batched form's autotuner on this grid and these fields: coordinate
         # descent over its choices, each timed with the L2 flushed and checked
         # against the FP64 direct sum (first field, 2,000 targets, 5e-6 bar)
@@ -625,8 +640,8 @@ def main():
                 "flops_counted": "algorithmic 4*F per pair (2 components x FMA x F fields); the hi/lo split "
                                  "executes 4x these on the tensor cores (W_hi,W_lo x T_hi,T_lo), plus padding",
                 # ncu dram__bytes_read.sum + dram__bytes_write.sum of one tc_leaf_kernel launch on the
-                # 655,362-cell, 64-field case (3.55 + 2.63 GB), scaled by the cell count
-                "traffic": 6.180e9 * g.n / 655362 if F == 64 else None,
+                # 655,362-cell, 64-field case (3.95 + 2.65 GB), scaled by the cell count
+                "traffic": 6.600e9 * g.n / 655362 if F == 64 else None,
                 "traffic_source": "ncu capture on 655,362 cells x 64 fields, scaled by cells",
                 "leaf_ms": leaf_ms, "proxy_ms": proxy_ms, "prep_upward_ms": up_ms}
     else:
@@ -670,7 +685,8 @@ def main():
             "work": {k: st[k] for k in ("pairs_pp", "pairs_pc", "pairs_cp", "pairs_cc", "macs_up", "macs_down",
                                         "macs_up_batched", "macs_down_batched")},
             "autotune": tuned,
-            "setup_s": {"grid_generation": t_gen, "tree_and_lists": t_lists, "plan_and_upload": st["setup_seconds"]},
+            "setup_s": {"grid_generation": t_gen, "tree_and_lists": t_lists, "plan_and_upload": st["setup_seconds"],
+                        "tree_and_lists_on_device": t_lists_dev, "device_build_list_equal": dev_build_same},
             "e2e": {"value": e2e_val, "unit": "evals/s", "h2d_bytes_per_step": 8 * g.n * F,
                     "d2h_bytes_per_step": 16 * g.n * F, "steps": e2e_steps,
                     "api": "sal_solve_host_async + sal_solve_host_wait (pinned host buffers, two staging slots)",

@@ -87,6 +87,19 @@ int sal_tree_destroy(sal_tree *t);
 int sal_dual_tree_traversal(const sal_tree *t, double theta, int32_t cluster_thresh, int32_t **list,
                             int64_t *count);
 
+/* tree_traverse and dual_tree_traversal with the refinement and the pair
+ * traversal on CUDA device `device`, for fast admission of new grids (no
+ * counterpart in the reference, which builds both on the host).  Results and
+ * order equal sal_tree_traverse and sal_dual_tree_traversal bit for bit: the
+ * per-point (xi, eta) and the panel radii and centres are computed with the
+ * host's libm, and MAC ratios within 1e-12 of theta are decided on the host.
+ * sal_dual_tree_traversal_device takes any tree (host- or device-built).  Both
+ * are synchronous and allocate their device scratch per call. */
+int sal_tree_traverse_device(const double *xs, const double *ys, const double *zs, int32_t point_count,
+                             int32_t cluster_thresh, int32_t device, sal_tree **out);
+int sal_dual_tree_traversal_device(const sal_tree *t, double theta, int32_t cluster_thresh, int32_t device,
+                                   int32_t **list, int64_t *count);
+
 /* single_tree_traversal, tree_module.f90:401-487.  *pc and *pp receive pairs
  * (index_target = point id, index_source = panel id); free with sal_free. */
 int sal_single_tree_traversal(const sal_tree *t, double theta, int32_t cluster_thresh, const double *xs,

@@ -107,6 +107,31 @@ extern "C" int sal_dual_tree_traversal(const sal_tree *t, double theta, int32_t 
     return SAL_OK;
 }
 
+extern "C" int sal_tree_traverse_device(const double *xs, const double *ys, const double *zs, int32_t n,
+                                        int32_t thresh, int32_t device, sal_tree **out) {
+    if (!xs || !ys || !zs || !out) return set_error(SAL_EINVAL, "null argument");
+    if (n < 0) return set_error(SAL_EINVAL, "negative point_count");
+    if (thresh < 2) return set_error(SAL_EINVAL, "cluster_thresh must be >= 2");
+    Tree *t = nullptr;
+    if (int rc = tree_build_device(xs, ys, zs, n, thresh, device, &t)) return rc;
+    sal_tree *s = new sal_tree();
+    static_cast<Tree &>(*s) = std::move(*t);
+    delete t;
+    *out = s;
+    return SAL_OK;
+}
+
+extern "C" int sal_dual_tree_traversal_device(const sal_tree *t, double theta, int32_t thresh, int32_t device,
+                                              int32_t **list, int64_t *count) {
+    if (!t || !list || !count) return set_error(SAL_EINVAL, "null argument");
+    std::vector<int32_t> L;
+    if (int rc = dual_tree_traversal_device(*t, theta, thresh, device, &L)) return rc;
+    *list = copy_out(L);
+    if (!*list) return set_error(SAL_ENOMEM, "out of host memory");
+    *count = (int64_t)(L.size() / 3);
+    return SAL_OK;
+}
+
 extern "C" int sal_single_tree_traversal(const sal_tree *t, double theta, int32_t thresh, const double *xs,
                                          const double *ys, const double *zs, int32_t own, int32_t **pc,
                                          int64_t *npc, int32_t **pp, int64_t *npp) {

@@ -274,6 +274,9 @@ extern "C" int sal_grid_create(const sal_tree *t_, const sal_grid_desc *d, sal_g
         delete G;
         return set_error(SAL_EINVAL, err);
     }
+    // grids made for 32-field blocks get the mma.sync groups now, so their
+    // stats count them; others build them if a tune switches to 32 fields
+    if (d->mode == SAL_MODE_DTT && d->max_fields <= 32) plan_build_mix(t, &g.plan);
     Plan &pl = g.plan;
     const int n = pl.n, P = pl.P, nd = pl.d + 1;
     g.nsrc = (int)pl.src_slot_panel.size();
@@ -358,6 +361,31 @@ extern "C" int sal_grid_destroy(sal_grid *G) {
     return SAL_OK;
 }
 
+// Device bytes ensure_mixed allocates for blocks of FT fields (the same
+// buffers, counted without allocating).
+static int64_t mixed_bytes_needed(const GridImpl &g, int FT) {
+    const Plan &pl = g.plan;
+    const bool tc = FT == 64 && !pl.tc_items.empty();
+    const int64_t P = pl.P, n = pl.n;
+    const int64_t nw = tc ? pl.n_wslots : g.nsrc, ndn = tc ? pl.n_dslots : g.ntgt;
+    const int64_t nunits_p = std::max<int64_t>(g.nproxy_units, pl.tc_nproxy_units);
+    auto vb = [](const auto &v) { return (int64_t)(v.size() * sizeof(v[0])); };
+    int64_t b = 4 * (int64_t)FT * ((n + nw * P) + ndn * 3 * P + (int64_t)g.nup * P + nunits_p * 3 * P) + 4 * n;
+    if (!tc) {
+        b += vb(pl.mix_leaf_groups) + vb(pl.mix_leaf_items) + vb(pl.mix_proxy_groups) + vb(pl.mix_proxy_items) +
+             vb(pl.mix_up_groups);
+    } else {
+        b += vb(pl.tc_leaf_groups) + vb(pl.tc_items) + vb(pl.tc_proxy_groups) + vb(pl.tc_proxy_items) +
+             vb(pl.tc_proxy_unit_beg) + vb(pl.tc_up_groups) + vb(pl.tc_up_items) + vb(pl.tc_up_unit_beg) +
+             vb(pl.tc_up_nodes) + vb(pl.tc_down_nodes) + vb(pl.m2m_tasks) + vb(pl.l2l_tasks) + vb(pl.tc_transfer);
+        const int64_t nbk = (int64_t)pl.tc_bas.size() / 3, nunits = pl.tc_up_unit_beg.empty() ? 0 : pl.tc_up_unit_beg.back();
+        b += 4 * nunits * P * FT + 4 * nbk * 16 * (pl.d + 1) + vb(pl.bsrc) + 4 * (int64_t)pl.bsrc.size() * 2 * FT +
+             (int64_t)sizeof(float4) * (n + (int64_t)g.nsrc * P) + (int64_t)sizeof(double2) * n +
+             4 * pl.tc_src_ksteps * 24;
+    }
+    return b;
+}
+
 extern "C" int sal_grid_stats_get(const sal_grid *G, sal_grid_stats *s) {
     if (!G || !s) return set_error(SAL_EINVAL, "null argument");
     const GridImpl &g = G->g;
@@ -379,15 +407,7 @@ extern "C" int sal_grid_stats_get(const sal_grid *G, sal_grid_stats *s) {
     s->setup_seconds = g.setup_seconds;
     s->macs_up_batched = pl.tc_items.empty() ? pl.macs_up : pl.tc_macs_up;
     s->macs_down_batched = pl.tc_items.empty() ? pl.macs_down : pl.tc_macs_down;
-    {
-        const int64_t FT = g.FT ? g.FT : (g.max_fields <= 32 ? 32 : 64), P = pl.P;
-        s->mixed_bytes = g.FT ? g.mix_bytes
-                              : 4 * FT * ((int64_t)pl.n + (int64_t)g.nsrc * P + 3 * P * (int64_t)g.ntgt + P * (int64_t)g.nup +
-                                          3 * P * (int64_t)g.nproxy_units) +
-                                    (int64_t)sizeof(MixGroup) * (int64_t)(pl.mix_leaf_groups.size() + pl.mix_proxy_groups.size() +
-                                                                          pl.mix_up_groups.size()) +
-                                    (int64_t)sizeof(Item) * (int64_t)(pl.mix_leaf_items.size() + pl.mix_proxy_items.size());
-    }
+    s->mixed_bytes = g.FT ? g.mix_bytes : mixed_bytes_needed(g, g.max_fields <= 32 ? 32 : 64);
     return SAL_OK;
 }
 
@@ -466,10 +486,11 @@ static void solve_fp64(GridImpl &g, const double *ssh, double *ox, double *oy, i
 static int ensure_mixed(GridImpl &g, int FT) {
     if (g.FT == FT) return SAL_OK;
     if (g.FT != 0) return set_error(SAL_EINVAL, "a grid's batched buffers are sized for one field block width");
+    const bool tc = FT == 64 && !g.plan.tc_items.empty();
+    if (!tc && !g.plan.mix_built && g.plan.mode == SAL_MODE_DTT) plan_build_mix(g.tree, &g.plan);
     const Plan &pl = g.plan;
     const size_t P = (size_t)pl.P, n = (size_t)pl.n;
     const int64_t before = g.bytes;
-    const bool tc = FT == 64 && !pl.tc_items.empty();
     // proxy-weight rows: source slots (and, in the tree passes, the other
     // panels below them); potential rows: target slots (and the panels below)
     const size_t nw = tc ? (size_t)pl.n_wslots : (size_t)g.nsrc, ndn = tc ? (size_t)pl.n_dslots : (size_t)g.ntgt;
@@ -484,11 +505,14 @@ static int ensure_mixed(GridImpl &g, int FT) {
         for (size_t p = 0; p < n; ++p) ip[(size_t)pl.perm[p]] = (int32_t)p;
         rc = upload_mix(g, &g.iperm, ip);
     }
-    if (!rc) rc = upload_mix(g, &g.mix_leaf_groups, pl.mix_leaf_groups);
-    if (!rc) rc = upload_mix(g, &g.mix_leaf_items, pl.mix_leaf_items);
-    if (!rc) rc = upload_mix(g, &g.mix_proxy_groups, pl.mix_proxy_groups);
-    if (!rc) rc = upload_mix(g, &g.mix_proxy_items, pl.mix_proxy_items);
-    if (!rc) rc = upload_mix(g, &g.mix_up_groups, pl.mix_up_groups);
+    if (!rc && !tc) {
+        // mma.sync passes
+        rc = upload_mix(g, &g.mix_leaf_groups, pl.mix_leaf_groups);
+        if (!rc) rc = upload_mix(g, &g.mix_leaf_items, pl.mix_leaf_items);
+        if (!rc) rc = upload_mix(g, &g.mix_proxy_groups, pl.mix_proxy_groups);
+        if (!rc) rc = upload_mix(g, &g.mix_proxy_items, pl.mix_proxy_items);
+        if (!rc) rc = upload_mix(g, &g.mix_up_groups, pl.mix_up_groups);
+    }
     if (!rc && tc) {
         // tcgen05 passes: items, split weight store, per-row source
         // coordinates, the per-point self pairs and the tree transfers
@@ -880,6 +904,7 @@ static int apply_tune(GridImpl &g, const sal_tune &t) {
     } else {
         g.plan.tc_opt.cta_groups = o.cta_groups;
     }
+    if (t.field_block == 32 && !g.plan.mix_built) plan_build_mix(g.tree, &g.plan);
     return SAL_OK;
 }
 

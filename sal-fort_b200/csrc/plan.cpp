@@ -310,11 +310,25 @@ bool plan_build(const Tree &t, int d, int mode, const int32_t *list, int64_t nli
         std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) { return ucost[a] > ucost[b]; });
         for (int32_t u : ord) pl->proxy_groups.push_back(units[u]);
     }
-    // ---------------------------------------------------------------- batched-form groups
-    // Same work as above, re-cut for the tensor-core kernels: items of at most
-    // kMixStage sources, groups of at most kMixRows targets, and a local
-    // coordinate origin per group (the panel centre) so the FP32 kernel tiles
-    // see small coordinate differences.
+    pl->leaf_panel = leaves;
+    pl->mix_built = false;
+    if (dtt && !plan_build_tc(t, pl, TcOptions{}, err)) return false;
+    // ---------------------------------------------------------------- point data in pool order
+    pl->pxi.resize(n); pl->peta.resize(n);
+    for (int32_t p = 0; p < n; ++p) { pl->pxi[p] = t.xi[t.order[p]]; pl->peta[p] = t.eta[t.order[p]]; }
+    return true;
+}
+
+// ---------------------------------------------------------------- 32-field groups
+// The batched form's work re-cut for the mma.sync kernels (32-field blocks):
+// items of at most kMixStage sources, groups of at most kMixRows targets, and
+// a local coordinate origin per group (the panel centre) so the FP32 kernel
+// tiles see small coordinate differences.  Built only for grids that use
+// 32-field blocks (plan_build leaves it out: it is a third of the plan's time).
+void plan_build_mix(const Tree &t, Plan *pl) {
+    const int P = pl->P;
+    const bool dtt = pl->mode == 0;
+    const std::vector<int32_t> &leaves = pl->leaf_panel;
     {
         auto rechunk = [&](const std::vector<Item> &src, int32_t ib, int32_t ie, std::vector<Item> &dst) {
             for (int32_t i = ib; i < ie; ++i) {
@@ -329,7 +343,6 @@ bool plan_build(const Tree &t, int d, int mode, const int32_t *list, int64_t nli
             }
         };
         pl->mix_leaf_groups.clear();
-        pl->tc_leaf_groups.clear();
         pl->mix_leaf_items.clear();
         if (dtt) {
             for (const Group &g : pl->leaf_groups) {
@@ -368,11 +381,7 @@ bool plan_build(const Tree &t, int d, int mode, const int32_t *list, int64_t nli
                 }
         }
     }
-    if (dtt && !plan_build_tc(t, pl, TcOptions{}, err)) return false;
-    // ---------------------------------------------------------------- point data in pool order
-    pl->pxi.resize(n); pl->peta.resize(n);
-    for (int32_t p = 0; p < n; ++p) { pl->pxi[p] = t.xi[t.order[p]]; pl->peta[p] = t.eta[t.order[p]]; }
-    return true;
+    pl->mix_built = true;
 }
 
 // ---------------------------------------------------------------- tcgen05 passes

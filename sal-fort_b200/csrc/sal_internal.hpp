@@ -47,7 +47,13 @@ Tree *tree_import(int32_t npanels, const int32_t *ints9, const double *dbl7, con
                   const int32_t *pt_idx, int32_t n, const double *xs, const double *ys, const double *zs,
                   std::string *err);
 void tree_set_points(Tree *t, const double *xs, const double *ys, const double *zs);
+void tree_finish_panels(Tree *t);   // radii and MAC centres from the panel bounds
+int dtt_decide(const Tree &t, int32_t it, int32_t is, double theta, int32_t thresh);
 std::vector<int32_t> dual_tree_traversal(const Tree &t, double theta, int32_t thresh);
+// The same two builds on a CUDA device (tree_dev.cu); SAL_* status codes.
+int tree_build_device(const double *xs, const double *ys, const double *zs, int32_t n, int32_t thresh, int device,
+                      Tree **out);
+int dual_tree_traversal_device(const Tree &t, double theta, int32_t thresh, int device, std::vector<int32_t> *L);
 void single_tree_traversal(const Tree &t, double theta, int32_t thresh, const double *xs, const double *ys,
                            const double *zs, int32_t own, std::vector<int32_t> *pc, std::vector<int32_t> *pp);
 int assign_points_to_panels(const Tree &t, const double *xs, const double *ys, const double *zs, int32_t own,
@@ -135,6 +141,8 @@ struct Plan {
     // batched form: items of at most kMixStage sources (DOWN items: rows of
     // a target slot's potentials, off = slot, cnt = rows, mask = first row)
     std::vector<MixGroup> mix_leaf_groups, mix_proxy_groups, mix_up_groups;
+    bool mix_built = false;                       // the three above and their items (plan_build_mix)
+    std::vector<int32_t> leaf_panel;              // leaf index (leaf_groups[].out) -> panel index
     // tcgen05 leaf pass: groups of at most kTcRows targets in pool order, their
     // items and the row map of the split weight store (per store row: wF row
     // if >= 0, phiF row -2-v if <= -2, zero row if -1; every leaf, source
@@ -192,6 +200,8 @@ bool plan_build(const Tree &t, int d, int mode, const int32_t *list, int64_t nli
                 const int32_t *pp, int64_t npp, Plan *plan, std::string *err);
 // (Re)builds the tcgen05 part of a DTT plan for the given options.
 bool plan_build_tc(const Tree &t, Plan *plan, const TcOptions &opt, std::string *err);
+// The 32-field (mma.sync) groups of the batched form, from a built plan.
+void plan_build_mix(const Tree &t, Plan *plan);
 
 constexpr int kMaxStage = 256;   // sources staged per item (items are split to fit)
 constexpr int kMixStage = 64;    // sources (or DOWN rows) staged per batched item

@@ -96,7 +96,7 @@ void tree_set_points(Tree *t, const double *xs, const double *ys, const double *
 }
 
 // Panel radius (tree_module.f90:224-244) and MAC centre.
-static void finish_panels(Tree *t) {
+void tree_finish_panels(Tree *t) {
     size_t np = t->p.size();
     t->cx.resize(np); t->cy.resize(np); t->cz.resize(np);
 #pragma omp parallel for schedule(static)
@@ -182,7 +182,7 @@ Tree *tree_build(const double *xs, const double *ys, const double *zs, int32_t n
             t->p.push_back(c);
         }
     }
-    finish_panels(t);
+    tree_finish_panels(t);
     return t;
 }
 
@@ -247,9 +247,24 @@ Tree *tree_import(int32_t np, const int32_t *I, const double *D, const int64_t *
     // the caller's radii are kept; only the MAC centres are derived here
     std::vector<double> radius(np);
     for (int32_t k = 0; k < np; ++k) radius[k] = t->p[k].radius;
-    finish_panels(t);
+    tree_finish_panels(t);
     for (int32_t k = 0; k < np; ++k) t->p[k].radius = radius[k];
     return t;
+}
+
+// One queued pair of dual_tree_traversal (tree_module.f90:300-392):
+// 0 an empty panel, 1..4 a list entry of type code - 1, 5 refine the
+// source, 6 refine the target.
+int dtt_decide(const Tree &t, int32_t it, int32_t is, double theta, int32_t thresh) {
+    const Panel &T = t.p[it - 1], &S = t.p[is - 1];
+    int64_t ct = T.count(), cs = S.count();
+    if (!(ct > 0 && cs > 0)) return 0;
+    double dist = clamp_acos(t.cx[it - 1] * t.cx[is - 1] + t.cy[it - 1] * t.cy[is - 1] + t.cz[it - 1] * t.cz[is - 1]);
+    double sep = (T.radius + S.radius) / dist;
+    if (dist > 0 && sep < theta) return 1 + (ct > thresh ? 2 : 0) + (cs > thresh ? 1 : 0);
+    if ((ct < thresh && cs < thresh) || (T.is_leaf && S.is_leaf)) return 1;
+    bool refine_source = T.is_leaf ? true : (S.is_leaf ? false : !(ct >= cs));
+    return refine_source ? 5 : 6;
 }
 
 // dual_tree_traversal, tree_module.f90:277-398: BFS over panel pairs seeded
@@ -260,21 +275,13 @@ std::vector<int32_t> dual_tree_traversal(const Tree &t, double theta, int32_t th
         for (int j = 1; j <= 6; ++j) { tq.push_back(i); sq.push_back(j); }
     for (size_t cur = 0; cur < tq.size(); ++cur) {
         int32_t it = tq[cur], is = sq[cur];
-        const Panel &T = t.p[it - 1], &S = t.p[is - 1];
-        int64_t ct = T.count(), cs = S.count();
-        if (!(ct > 0 && cs > 0)) continue;
-        double dist = clamp_acos(t.cx[it - 1] * t.cx[is - 1] + t.cy[it - 1] * t.cy[is - 1] + t.cz[it - 1] * t.cz[is - 1]);
-        double sep = (T.radius + S.radius) / dist;
-        if (dist > 0 && sep < theta) {
-            int ty = (ct > thresh ? 2 : 0) + (cs > thresh ? 1 : 0);
-            L.insert(L.end(), {it, is, ty});
-        } else if ((ct < thresh && cs < thresh) || (T.is_leaf && S.is_leaf)) {
-            L.insert(L.end(), {it, is, 0});
-        } else {
-            bool refine_source = T.is_leaf ? true : (S.is_leaf ? false : !(ct >= cs));
-            for (int c = 0; c < 4; ++c) {
-                if (refine_source) { tq.push_back(it); sq.push_back(S.child[c]); }
-                else { tq.push_back(T.child[c]); sq.push_back(is); }
+        const int c = dtt_decide(t, it, is, theta, thresh);
+        if (c >= 1 && c <= 4) {
+            L.insert(L.end(), {it, is, c - 1});
+        } else if (c >= 5) {
+            for (int k = 0; k < 4; ++k) {
+                if (c == 5) { tq.push_back(it); sq.push_back(t.p[is - 1].child[k]); }
+                else { tq.push_back(t.p[it - 1].child[k]); sq.push_back(is); }
             }
         }
     }

@@ -40,7 +40,7 @@ EXPORTS = (
     "sal_solve_host_wait", "sal_grid_set_graphs", "sal_grid_inject_timeout", "sal_fast_sum",
     "sal_mom6_proxy_source_compute", "sal_mom6_pc_compute", "sal_mom6_pp_compute", "sal_dropin_config",
     "sal_dropin_release", "sal_grid_tune_get", "sal_grid_tune_set", "sal_grid_autotune", "sal_read_values",
-    "sal_write_values", "sal_solve_joint",
+    "sal_write_values", "sal_solve_joint", "sal_tree_traverse_device", "sal_dual_tree_traversal_device",
 )
 
 
@@ -110,6 +110,8 @@ def lib():
         L.sal_tree_export.argtypes = [vp, vp, vp, vp, vp]
         L.sal_tree_destroy.argtypes = [vp]
         L.sal_dual_tree_traversal.argtypes = [vp, d, i32, C.POINTER(C.POINTER(i32)), C.POINTER(i64)]
+        L.sal_tree_traverse_device.argtypes = [vp, vp, vp, i32, i32, i32, pp_]
+        L.sal_dual_tree_traversal_device.argtypes = [vp, d, i32, i32, C.POINTER(C.POINTER(i32)), C.POINTER(i64)]
         L.sal_single_tree_traversal.argtypes = [vp, d, i32, vp, vp, vp, i32, C.POINTER(C.POINTER(i32)),
                                                 C.POINTER(i64), C.POINTER(C.POINTER(i32)), C.POINTER(i64)]
         L.sal_assign_points_to_panels.argtypes = [vp, vp, vp, vp, i32, vp, i32]
@@ -209,13 +211,19 @@ class Tree:
         return e["pt_idx"][e["pt_off"][k - 1]:e["pt_off"][k]]
 
 
-def tree_traverse(xs, ys, zs, point_count, cluster_thresh) -> Tree:
-    """tree_module.f90:59-246."""
+def tree_traverse(xs, ys, zs, point_count, cluster_thresh, device=None) -> Tree:
+    """tree_module.f90:59-246.  device: None builds on the host; a CUDA
+    ordinal refines on that device (the same tree, bit for bit)."""
     xs, ys, zs = _f64(xs), _f64(ys), _f64(zs)
     if len(xs) != point_count:
         raise ValueError("point_count differs from len(xs)")
     h = C.c_void_p()
-    _check(lib().sal_tree_traverse(_ptr(xs), _ptr(ys), _ptr(zs), int(point_count), int(cluster_thresh), C.byref(h)))
+    if device is None:
+        _check(lib().sal_tree_traverse(_ptr(xs), _ptr(ys), _ptr(zs), int(point_count), int(cluster_thresh),
+                                       C.byref(h)))
+    else:
+        _check(lib().sal_tree_traverse_device(_ptr(xs), _ptr(ys), _ptr(zs), int(point_count), int(cluster_thresh),
+                                              int(device), C.byref(h)))
     return Tree(h.value, point_count)
 
 
@@ -241,10 +249,16 @@ def _take_list(p, count, width):
     return out
 
 
-def dual_tree_traversal(tree: Tree, theta, cluster_thresh) -> np.ndarray:
-    """tree_module.f90:277-398: (n, 3) int32 of (index_target, index_source, interact_type)."""
+def dual_tree_traversal(tree: Tree, theta, cluster_thresh, device=None) -> np.ndarray:
+    """tree_module.f90:277-398: (n, 3) int32 of (index_target, index_source, interact_type).
+    device: None traverses on the host, else on that CUDA device (the same list)."""
     p, cnt = C.POINTER(C.c_int32)(), C.c_int64()
-    _check(lib().sal_dual_tree_traversal(tree.handle, float(theta), int(cluster_thresh), C.byref(p), C.byref(cnt)))
+    if device is None:
+        _check(lib().sal_dual_tree_traversal(tree.handle, float(theta), int(cluster_thresh), C.byref(p),
+                                             C.byref(cnt)))
+    else:
+        _check(lib().sal_dual_tree_traversal_device(tree.handle, float(theta), int(cluster_thresh), int(device),
+                                                    C.byref(p), C.byref(cnt)))
     return _take_list(p, cnt, 3)
 
 

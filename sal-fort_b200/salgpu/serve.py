@@ -121,7 +121,8 @@ class Server:
     """Resident grids + per-grid continuous batching on CUDA streams."""
 
     def __init__(self, hbm_budget_bytes: int, max_batch: int = 64, device: int = 0, clock=time.perf_counter,
-                 grid_factory=Grid, priorities: bool = True, patience: float = 2.0, graphs: bool = False):
+                 grid_factory=Grid, priorities: bool = True, patience: float = 2.0, graphs: bool = False,
+                 device_setup: bool = True):
         try:
             import torch
         except ImportError:           # the CPU test double needs no torch
@@ -140,14 +141,18 @@ class Server:
         self.priorities = priorities
         self.patience = float(patience)
         self.graphs = graphs                 # one CUDA graph per (grid, batch width)
+        self.device_setup = device_setup     # tree and list built on the device when one is present
         self.batches: list[tuple] = []     # (grid, fields, launch time, done time) of finished batches
 
     # ------------------------------------------------------------------ grids
     def register_grid(self, spec: GridSpec) -> None:
-        """Builds the host tree and lists of a grid (tree_module.f90) once; the
-        device plan is created on admission."""
-        tree = tree_traverse(spec.xs, spec.ys, spec.zs, len(spec.xs), spec.thresh)
-        inter = dual_tree_traversal(tree, spec.theta, spec.thresh)
+        """Builds the tree and lists of a grid (tree_module.f90) once, on the
+        device when there is one and device_setup is set; the device plan is
+        created on admission."""
+        on_dev = self.device_setup and self.torch is not None and self.torch.cuda.is_available()
+        dev = self.device if on_dev else None
+        tree = tree_traverse(spec.xs, spec.ys, spec.zs, len(spec.xs), spec.thresh, device=dev)
+        inter = dual_tree_traversal(tree, spec.theta, spec.thresh, device=dev)
         self.grids[spec.name] = _Resident(spec, tree, inter)
 
     def _bytes_needed(self, r: _Resident, g: Grid) -> int:

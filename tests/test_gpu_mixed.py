@@ -262,3 +262,19 @@ def test_joint_solve_of_uneven_grids_equals_separate_solves():
     g9 = _grid("small_3000", 20, 3, seed=21, degree=9)[3]
     with pytest.raises(S.SalError):
         S.solve_joint([grids[0], g9], [sshs[0], sshs[0]])
+
+
+@pytest.mark.parametrize("nfields", [64, 32])
+def test_mixed_bytes_estimate_equals_the_allocation(nfields):
+    """stats()["mixed_bytes"] before the first batched solve (what the serving
+    loop budgets with) equals what that solve allocates, for 64-field
+    (tcgen05) and 32-field (mma.sync) blocks."""
+    torch = _torch()
+    S, g, hs, grid = _grid("cfg0", 100, nfields)
+    est = grid.stats()["mixed_bytes"]
+    before = grid.stats()["device_bytes"]
+    grid.solve(torch.tensor(hs, device="cuda"), form=S.FORM_MIXED)
+    torch.cuda.synchronize()
+    st = grid.stats()
+    assert st["mixed_bytes"] == est
+    assert st["device_bytes"] - before == est
