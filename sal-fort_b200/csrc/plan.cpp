@@ -605,7 +605,7 @@ bool plan_build_tc(const Tree &t, Plan *pl, const TcOptions &opt, std::string *e
                     const int32_t l = leaf_of_pos[b];
                     const Panel &q = t.p[leaves[l]];
                     const int64_t le = std::min<int64_t>(e, q.end);
-                    if ((b - q.begin) % 8 != 0) { *err = "internal: point range starts inside a leaf"; return false; }
+                    if ((b - q.begin) % 8 != 0) return false;   // a point range starting inside a leaf
                     push(0, b, le - b, leaf_b[l] + (b - q.begin), leaves[l]);
                     b = le;
                 }
@@ -629,17 +629,50 @@ bool plan_build_tc(const Tree &t, Plan *pl, const TcOptions &opt, std::string *e
         return true;
     };
 
+    // Many work lists at once, on every host thread: job j's items land in
+    // dst[range[j].first, range[j].second), the jobs in order.
+    struct Job {
+        int32_t ib, ie, kt, extra;
+    };
+    auto convert_all = [&](const std::vector<Item> &src, const std::vector<Job> &jobs, std::vector<TcItem> &dst,
+                           std::vector<std::pair<int32_t, int32_t>> &range) -> bool {
+        const int64_t nj = (int64_t)jobs.size();
+        std::vector<std::vector<TcItem>> part(nj);
+        int bad = 0;
+#pragma omp parallel for schedule(dynamic, 32) reduction(| : bad)
+        for (int64_t j = 0; j < nj; ++j)
+            if (!convert(src, jobs[j].ib, jobs[j].ie, jobs[j].kt, part[j], jobs[j].extra)) bad |= 1;
+        if (bad) { *err = "internal: point range starts inside a leaf"; return false; }
+        std::vector<int64_t> off(nj + 1, (int64_t)dst.size());
+        for (int64_t j = 0; j < nj; ++j) off[j + 1] = off[j] + (int64_t)part[j].size();
+        if (off[nj] > INT32_MAX) { *err = "tcgen05 work list too long"; return false; }
+        dst.resize((size_t)off[nj]);
+        range.resize(nj);
+#pragma omp parallel for schedule(dynamic, 32)
+        for (int64_t j = 0; j < nj; ++j) {
+            std::copy(part[j].begin(), part[j].end(), dst.begin() + off[j]);
+            range[j] = {(int32_t)off[j], (int32_t)off[j + 1]};
+        }
+        return true;
+    };
+
     // ---- leaf pass: groups of at most kTcRows targets in pool order
     std::vector<int32_t> gord(pl->leaf_groups.size());
     std::iota(gord.begin(), gord.end(), 0);
     std::sort(gord.begin(), gord.end(), [&](int a, int b) { return pl->leaf_groups[a].tgt < pl->leaf_groups[b].tgt; });
     pl->tc_macs_down = 0;
+    std::vector<Job> jobs;
+    std::vector<std::pair<int32_t, int32_t>> range;
+    jobs.reserve(gord.size());
     for (int32_t gi : gord) {
         const Group &g = pl->leaf_groups[gi];
+        jobs.push_back(Job{g.ib, g.ie, leaves[g.out], tree ? g.out : -1});
+    }
+    if (!convert_all(pl->leaf_items, jobs, pl->tc_items, range)) return false;
+    for (size_t x = 0; x < gord.size(); ++x) {
+        const Group &g = pl->leaf_groups[gord[x]];
         const int kt = leaves[g.out];
-        const int32_t ib = (int32_t)pl->tc_items.size();
-        if (!convert(pl->leaf_items, g.ib, g.ie, kt, pl->tc_items, tree ? g.out : -1)) return false;
-        const int32_t ie = (int32_t)pl->tc_items.size();
+        const int32_t ib = range[x].first, ie = range[x].second;
         if (tree && leaf_phi_block[g.out] >= 0) pl->tc_macs_down += (double)g.nt * P;
         for (int32_t r = 0; r < g.nt; r += kTcRows) {
             MixGroup m{};
@@ -677,12 +710,14 @@ bool plan_build_tc(const Tree &t, Plan *pl, const TcOptions &opt, std::string *e
         std::vector<int32_t> ord(units.size());
         std::iota(ord.begin(), ord.end(), 0);
         std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) { return units[a].cost > units[b].cost; });
-        for (int32_t uo : ord) {
+        jobs.clear();
+        for (int32_t uo : ord) jobs.push_back(Job{units[uo].ib, units[uo].ie, pl->tgt_slot_panel[units[uo].slot], -1});
+        if (!convert_all(pl->proxy_items, jobs, pl->tc_proxy_items, range)) return false;
+        for (size_t x = 0; x < ord.size(); ++x) {
+            const int32_t uo = ord[x];
             const U &u = units[uo];
             const int kt = pl->tgt_slot_panel[u.slot];
-            const int32_t ib = (int32_t)pl->tc_proxy_items.size();
-            if (!convert(pl->proxy_items, u.ib, u.ie, kt, pl->tc_proxy_items, -1)) return false;
-            const int32_t ie = (int32_t)pl->tc_proxy_items.size();
+            const int32_t ib = range[x].first, ie = range[x].second;
             for (int32_t r = 0; r < P; r += kTcProxyRows) {
                 MixGroup m{};
                 m.tgt = u.slot; m.nt = std::min(kTcProxyRows, P - r); m.ib = ib; m.ie = ie; m.out = uo; m.row0 = r;
@@ -705,7 +740,7 @@ bool plan_build_tc(const Tree &t, Plan *pl, const TcOptions &opt, std::string *e
     auto add_unit = [&](int ks, int64_t b, int64_t e, int32_t out, int32_t nodes_slot) -> bool {
         const std::vector<Item> range{Item{(int32_t)b, (int32_t)(e - b), -1, 0}};
         const int32_t ib = (int32_t)pl->tc_up_items.size();
-        if (!convert(range, 0, 1, ks, pl->tc_up_items, -1)) return false;
+        if (!convert(range, 0, 1, ks, pl->tc_up_items, -1)) { *err = "internal: point range starts inside a leaf"; return false; }
         const int32_t ie = (int32_t)pl->tc_up_items.size();
         for (int32_t i = ib; i < ie; ++i) {
             TcItem &r = pl->tc_up_items[i];
