@@ -155,6 +155,8 @@ typedef struct {
     int32_t proxy_unit_kpairs;  /* proxy pass: kernel pairs per work unit, in units of 1024 */
     int32_t cta_groups;         /* tcgen05 launches: target groups one CTA walks at most */
     int32_t field_block;        /* fields per block: 64 (tcgen05 passes) or 32 (mma.sync passes) */
+    int32_t f16;                /* 64-field leaf pass: 1 FP16 hi/lo operands (16 sources per MMA), scaled per field and
+                                   per target by powers of two; 0 TF32 hi/lo (8 sources per MMA) */
 } sal_tune;
 
 /* Flattens the tree and lists into device-resident arrays (once per grid). */

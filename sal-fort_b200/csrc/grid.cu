@@ -74,6 +74,9 @@ struct GridImpl {
     float *basis = nullptr;           // upward pass: per-point BLI factors per basis k-step
     int32_t *bsrc = nullptr;
     float *bstore = nullptr;          // split weight store of the tcgen05 leaf pass
+    void *bstore16 = nullptr;         // FP16 leaf pass: its FP16 hi/lo weight store (one spare unit at the end)
+    float *tscale = nullptr, *tinv = nullptr;   // FP16 leaf pass: per target, its kernel values' scale
+    unsigned *fmax = nullptr;         // FP16 leaf pass: the block's field maxima (source weights, potentials)
     float4 *sloc = nullptr;
     float *sxyz = nullptr;
     int32_t *iperm = nullptr;         // caller index -> pool position
@@ -382,6 +385,7 @@ static int64_t mixed_bytes_needed(const GridImpl &g, int FT) {
         b += 4 * nunits * P * FT + 4 * nbk * 16 * (pl.d + 1) + vb(pl.bsrc) + 4 * (int64_t)pl.bsrc.size() * 2 * FT +
              (int64_t)sizeof(float4) * (n + (int64_t)g.nsrc * P) + (int64_t)sizeof(double2) * n +
              4 * pl.tc_src_ksteps * 24;
+        if (pl.tc_opt.f16) b += ((int64_t)pl.bsrc.size() / 8 + 1) * 2048 + 128 * 4 + 2 * 4 * n;
     }
     return b;
 }
@@ -482,6 +486,8 @@ static void solve_fp64(GridImpl &g, const double *ssh, double *ox, double *oy, i
     }
 }
 
+static mix::TcArgs leaf_args(GridImpl &g, double *ox, double *oy, int64_t ld_out, int f0, int nf);
+
 // Device buffers of the batched form, sized for blocks of FT fields.
 static int ensure_mixed(GridImpl &g, int FT) {
     if (g.FT == FT) return SAL_OK;
@@ -574,6 +580,23 @@ static int ensure_mixed(GridImpl &g, int FT) {
             if (dc) cudaFree(dc);
             if (e != cudaSuccess) return set_error(SAL_ECUDA, std::string("batched set-up: ") + cudaGetErrorString(e));
         }
+        if (!rc && pl.tc_opt.f16) {
+            // FP16 leaf pass: its weight store (zeroed: the spare unit past the
+            // last item must hold finite values), field maxima, and the
+            // per-target scales of the kernel values, once per plan
+            const size_t units = pl.bsrc.size() / 8 + 1;
+            rc = malloc_mix(g, reinterpret_cast<unsigned char **>(&g.bstore16), units * 2048);
+            if (!rc) rc = malloc_mix(g, &g.fmax, (size_t)128);
+            if (!rc) rc = malloc_mix(g, &g.tscale, n);
+            if (!rc) rc = malloc_mix(g, &g.tinv, n);
+            if (!rc) {
+                CK(cudaMemsetAsync(g.bstore16, 0, units * 2048, g.stream));
+                mix::TcArgs t = leaf_args(g, nullptr, nullptr, 0, 0, 0);
+                mix::launch_target_scales(t, g.tscale, g.tinv, g.stream);
+                CK(cudaStreamSynchronize(g.stream));
+                CK(cudaGetLastError());
+            }
+        }
         if (!rc) CK(cudaDeviceGetAttribute(&g.nsm, cudaDevAttrMultiProcessorCount, g.dev));
     }
     if (rc) {
@@ -607,6 +630,12 @@ static mix::TcArgs leaf_args(GridImpl &g, double *ox, double *oy, int64_t ld_out
     t.ld_out = ld_out;
     t.f0 = f0;
     t.nf = nf;
+    if (g.bstore16) {
+        t.bstore16 = g.bstore16;
+        t.tscale = g.tscale;
+        t.tinv = g.tinv;
+        t.fmax = g.fmax;
+    }
     return t;
 }
 
@@ -700,10 +729,20 @@ static void solve_mixed_block(GridImpl &g, const double *ssh, int64_t ld_ssh, in
         mix::launch_finalize_mix(g.proxy_unit_beg, g.mix_proxy_partial, g.ntgt, 3 * P, FT, g.phiF, st);
     }
     if (timed) cudaEventRecord(g.ev[2], st);
+    // the leaf pass's weight rows: TF32 (the potential rows: the points' and
+    // proxies' rows are in place), or FP16 (every row, scaled per field)
+    auto leaf_store = [&]() {
+        if (g.bstore16) {
+            cudaMemsetAsync(g.fmax, 0, 128 * sizeof(unsigned), st);
+            mix::launch_field_max(g.bsrc, (int64_t)pl.bsrc.size() / 8, g.wF, g.phiF, g.fmax, st);
+            mix::launch_split_store16(g.bsrc, (int64_t)pl.bsrc.size() / 8, g.wF, g.phiF, g.fmax, g.bstore16, st);
+        } else {
+            mix::launch_split_store(g.bsrc, pl.tc_src_ksteps, (int64_t)pl.bsrc.size() / 8, g.wF, g.phiF, g.bstore, st);
+        }
+    };
     if (joint) {
-        // the potential rows of the split weight store; the caller runs the
-        // leaf pass, jointly with other grids'
-        mix::launch_split_store(g.bsrc, pl.tc_src_ksteps, (int64_t)pl.bsrc.size() / 8, g.wF, g.phiF, g.bstore, st);
+        // the caller runs the leaf pass, jointly with other grids'
+        leaf_store();
         *joint = leaf_args(g, ox, oy, ld_out, f0, nf);
         return;
     }
@@ -711,9 +750,8 @@ static void solve_mixed_block(GridImpl &g, const double *ssh, int64_t ld_ssh, in
     a.tgt = g.pool;
     a.tgt_nodes = g.tgt_nodes;
     if (g.bstore) {
-        // 64-field blocks: the potential rows of the split weight store, then
-        // the tcgen05 leaf pass
-        mix::launch_split_store(g.bsrc, pl.tc_src_ksteps, (int64_t)pl.bsrc.size() / 8, g.wF, g.phiF, g.bstore, st);
+        // 64-field blocks: the leaf pass's weight rows, then the tcgen05 leaf pass
+        leaf_store();
         mix::launch_tc_leaf(leaf_args(g, ox, oy, ld_out, f0, nf), g.nsm, cg, g.err, st);
     } else {
         a.groups = g.mix_leaf_groups;
@@ -785,6 +823,8 @@ extern "C" int sal_solve_joint(sal_grid *const *grids, int32_t ngrids, const dou
             return set_error(SAL_EINVAL, "the grids of a joint solve share one device and one degree");
         if (g.max_fields <= 32 || g.plan.tc_items.empty())
             return set_error(SAL_EINVAL, "a joint solve needs grids with 64-field blocks (max_fields > 32)");
+        if (g.plan.tc_opt.f16 != grids[0]->g.plan.tc_opt.f16)
+            return set_error(SAL_EINVAL, "the grids of a joint solve share one leaf-pass precision (sal_tune.f16)");
     }
     CK(cudaSetDevice(grids[0]->g.dev));
     for (int k = 0; k < ngrids; ++k) {
@@ -875,6 +915,7 @@ static sal_tune tune_of(const GridImpl &g) {
     t.proxy_unit_kpairs = o.proxy_unit_kpairs;
     t.cta_groups = o.cta_groups;
     t.field_block = g.FT ? g.FT : (g.max_fields <= 32 ? 32 : 64);
+    t.f16 = o.f16;
     return t;
 }
 
@@ -886,9 +927,11 @@ static int apply_tune(GridImpl &g, const sal_tune &t) {
     o.up_chunk = t.up_chunk;
     o.proxy_unit_kpairs = t.proxy_unit_kpairs;
     o.cta_groups = t.cta_groups;
+    o.f16 = t.f16 ? 1 : 0;
     const TcOptions &c = g.plan.tc_opt;
     const bool same_plan = o.chain_ksteps == c.chain_ksteps && o.tree_passes == c.tree_passes &&
-                           o.up_chunk == c.up_chunk && o.proxy_unit_kpairs == c.proxy_unit_kpairs;
+                           o.up_chunk == c.up_chunk && o.proxy_unit_kpairs == c.proxy_unit_kpairs &&
+                           o.f16 == c.f16;
     const int cur_block = g.FT ? g.FT : (g.max_fields <= 32 ? 32 : 64);
     if (same_plan && t.field_block == cur_block) {
         if (o.cta_groups < 1) return set_error(SAL_EINVAL, "tcgen05 options must be positive");
@@ -1035,6 +1078,7 @@ extern "C" int sal_grid_autotune(sal_grid *G, const double *ssh, int32_t nf, int
     struct Axis { int32_t sal_tune::*field; std::vector<int32_t> values; };
     const std::vector<Axis> axes = {
         {&sal_tune::tree_passes, {1, 0}},
+        {&sal_tune::f16, {0, 1}},
         {&sal_tune::chain_ksteps, {8, 16, 32, 64}},
         {&sal_tune::cta_groups, {1, 2, 4}},
         {&sal_tune::proxy_unit_kpairs, {324, 648, 1296}},

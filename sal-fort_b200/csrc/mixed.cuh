@@ -66,6 +66,13 @@ struct TcArgs {
     int f0, nf;
     float *partial;           // proxy / upward pass: per-unit rows (P x components x 64 fields)
     const float *basis;       // upward pass: BLI factors per basis k-step
+    // FP16 leaf pass (bstore16 non-null): the FP16 hi/lo weight store (2 KB
+    // per unit of 8 rows), per target its kernel-value scale and inverse, and
+    // the block's field maxima (as float bits): 64 of source weights, then 64
+    // of potentials
+    const void *bstore16;
+    const float *tscale, *tinv;
+    const unsigned *fmax;
 };
 // cta_groups: groups one CTA walks at most (the grid has every SM busy
 // otherwise)
@@ -85,6 +92,16 @@ void launch_basis_store(const int32_t *bas, int64_t nbk, const double2 *xieta, c
 size_t tc_smem_bytes();
 void launch_split_store(const int32_t *bsrc, int64_t k0, int64_t k1, const float *wF, const float *phiF,
                         float *bstore, cudaStream_t st);
+// FP16 leaf pass: per field the largest |value| of the split store's source
+// weight rows and potential rows (units [0, nunits)) into fmax[f] and
+// fmax[64 + f] (float bits; fmax zeroed first); the FP16 hi/lo store of
+// those units with those scales; per target the scale of its kernel values
+// (once per plan).
+void launch_field_max(const int32_t *bsrc, int64_t nunits, const float *wF, const float *phiF, unsigned *fmax,
+                      cudaStream_t st);
+void launch_split_store16(const int32_t *bsrc, int64_t nunits, const float *wF, const float *phiF,
+                          const unsigned *fmax, void *bstore16, cudaStream_t st);
+void launch_target_scales(const TcArgs &a, float *tscale, float *tinv, cudaStream_t st);
 void launch_source_local(const double4 *pool, const int2 *ranges, const double4 *centres, int nranges, float4 *sloc,
                          cudaStream_t st);
 void launch_self_pair(const double4 *pool, int n, double2 *selfk, cudaStream_t st);

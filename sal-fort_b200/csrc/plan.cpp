@@ -620,11 +620,14 @@ bool plan_build_tc(const Tree &t, Plan *pl, const TcOptions &opt, std::string *e
             push(2, dslot[leaves[extra_down_leaf]], 3 * P, phi_b0 + (int64_t)leaf_phi_block[extra_down_leaf] * P38, -1);
         const int32_t ie = (int32_t)dst.size();
         // accumulator chains: end one after the item that brings it to
-        // chain_ksteps k-steps, and always after the list's last item
+        // chain_ksteps k-steps, and always after the list's last item.  The
+        // FP16 leaf pass scales kernel tiles and interpolation rows apart, so
+        // there DOWN items form chains of their own.
         for (int32_t i = ib, chain = 0; i < ie; ++i) {
             TcItem &r = dst[i];
             chain += (r.cnt + 7) / 8;
-            if (chain >= opt.chain_ksteps || i == ie - 1) { r.kind |= kTcFlush; chain = 0; }
+            const bool kind_changes = opt.f16 && i + 1 < ie && ((r.kind & 3) == 2) != ((dst[i + 1].kind & 3) == 2);
+            if (chain >= opt.chain_ksteps || i == ie - 1 || kind_changes) { r.kind |= kTcFlush; chain = 0; }
         }
         return true;
     };

@@ -114,6 +114,8 @@ struct TcOptions {
     int32_t up_chunk = 4096;            // direct upward pass: points per work unit at least
     int32_t proxy_unit_kpairs = 648;    // proxy pass: kernel pairs of a work unit, in units of 1024
     int32_t cta_groups = 1;             // tcgen05 launches: groups a CTA walks at most
+    int32_t f16 = 0;                    // leaf pass: 1: FP16 hi/lo operands (kind::f16, 16 sources per MMA)
+                                        //    with power-of-two scales; 0: TF32 hi/lo (8 sources per MMA)
 };
 
 struct Plan {

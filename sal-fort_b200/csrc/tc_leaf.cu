@@ -35,6 +35,17 @@
 //               prefetches the next item's tiles into L2.
 //   warps 10-13 fold finished accumulator chains into the running sums and
 //               write the outputs (warp w: tensor memory lanes 32(w%4)..+31).
+// FP16 leaf pass (sal_tune.f16): the same machine with kind::f16 MMAs, 16
+// sources per MMA.  A stage is 64 sources (eight units of 8, the split
+// store's granularity; an odd unit count is completed with a zero unit);
+// kernel tiles and weight tiles are FP16 hi + lo (11 + 11 bits, as TF32 hi +
+// lo), in the same shared-memory bytes, so each stage carries twice the
+// sources for the same MMA count and stores.  FP16's range needs scales:
+// every target's kernel values are multiplied by a power of two that takes
+// its largest one (computed once per plan) to at most 2^12, every field's
+// source weights and its potentials by powers of two of their own (per
+// solve), and the fold divides them out of each chain; DOWN items (O(1)
+// interpolation weights against potentials) form chains of their own.
 // The tensor cores accumulate with truncation, so one chain over all of a
 // target's sources would bias the result toward zero: a chain ends after about
 // 32 k-steps (plan flag kTcFlush) and is folded into the group's running sums
@@ -43,6 +54,8 @@
 // (columns 0-255); shared memory holds only the operand rings.  The next chain
 // starts once the fold warps have read the accumulator; the two-stage
 // kernel-tile ring lets the producers run on meanwhile.
+#include <cuda_fp16.h>
+#include <algorithm>
 #include <cuda_runtime.h>
 
 #include "kernels.cuh"
@@ -80,6 +93,15 @@ static_assert(kTcChunk % kStageK == 0, "items are whole stages");
 // instruction descriptor: D F32, A/B TF32, both K-major, N = 256, M = 128
 constexpr uint32_t kIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(256 >> 3) << 17) |
                             ((uint32_t)(128 >> 4) << 24);
+// the same for kind::f16 with A/B FP16 (format 0), 16 sources per MMA
+constexpr uint32_t kIdescF16 = (1u << 4) | ((uint32_t)(256 >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+// FP16 leaf pass: a stage is 64 sources, eight units of 8 (a unit is one
+// TF32 k-step: the split store's granularity); a unit of the FP16 weight store
+// is 128 rows x 8 halves, 8-row groups 128 B apart (2 KB)
+constexpr int kStageKF16 = 64;
+constexpr int kW16UnitBytes = 2048;
+// FP16 operands are scaled by powers of two to at most 2^12 (FP16 max 65504)
+constexpr int kF16TopExp = 12;
 
 struct TcSmem {
     float Kt[kKStages][kStageKs][2][kTileFloats];   // per stage: k-step x {hi, lo} x 256 rows x 8
@@ -173,6 +195,40 @@ __device__ __forceinline__ void mma_ss(uint32_t d_tmem, uint64_t a, uint64_t b, 
         "l"(a), "l"(b), "r"(kIdesc), "r"(accumulate)
         : "memory");
 }
+// D[tmem] (+)= A[smem] * B[smem], FP16 operands, 16 sources
+__device__ __forceinline__ void mma_ss_f16(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d_tmem),
+        "l"(a), "l"(b), "r"(kIdescF16), "r"(accumulate)
+        : "memory");
+}
+// Descriptor of an FP16 weight tile of two store units (16 sources): K core
+// matrices one unit (2 KB) apart, 8-row groups 128 B apart.
+__device__ __forceinline__ uint64_t smem_desc_w16(const void *p) {
+    const uint64_t addr = smem_u32(p);
+    return ((addr >> 4) & 0x3FFFull) | ((uint64_t)(kW16UnitBytes >> 4) << 16) | ((uint64_t)(128 >> 4) << 32) |
+           (1ull << 46);
+}
+// FP16 hi + lo of two values, packed as half2 words: hi = round(v), lo = round(v - hi)
+__device__ __forceinline__ void split_f16x2(float a, float b, uint32_t &hi, uint32_t &lo) {
+    const __half2 h = __floats2half2_rn(a, b);
+    const float2 back = __half22float2(h);
+    const __half2 l = __floats2half2_rn(a - back.x, b - back.y);
+    hi = *reinterpret_cast<const uint32_t *>(&h);
+    lo = *reinterpret_cast<const uint32_t *>(&l);
+}
+// The power of two that takes a magnitude m to at most 2^kF16TopExp (1 for
+// m = 0), and its inverse.
+__host__ __device__ inline float f16_scale(float m) {
+    if (!(m > 0.f)) return 1.f;
+    int e;
+    frexpf(m, &e);   // m < 2^e
+    e = kF16TopExp - e;
+    e = e < -120 ? -120 : (e > 120 ? 120 : e);
+    return ldexpf(1.f, e);
+}
+
 __device__ __forceinline__ void mma_commit(uint64_t *bar) {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
                  : "memory");
@@ -269,11 +325,30 @@ __device__ __forceinline__ void emit_chunk(const float (&x)[16], int c0, int f, 
 // ends go to the caller's outputs.  MODE 1 (proxy): columns 85c + r are
 // Cartesian component c of proxy r, ends go to the unit's partial rows `part`.
 // MODE 2 (upward): columns j < 128 are proxies row0 + j.
+//
+// FP16 leaf pass (scaled, the same in every lane): the chain's operands were
+// scaled by powers of two, the weight rows of field f by 1 / fsc and the
+// kernel tile's column of target t by 1 / csc[tgt + t] (csc null: DOWN
+// chains, unscaled columns); the fold multiplies the chain by fsc * csc
+// first (exact: powers of two).
 template <int MODE>
 __device__ __noinline__ void fold_chain(uint32_t td, int q, int lane, bool end, bool first, int tgt, int nt,
                                         const int32_t *__restrict__ perm, double *out_x, double *out_y,
-                                        int64_t ld_out, int f0, int nf, bool skip, float *part) {
+                                        int64_t ld_out, int f0, int nf, bool skip, float *part, bool scaled = false,
+                                        float fsc = 1.f, const float *__restrict__ csc = nullptr) {
     const int f = 16 * q + (lane & 15), odd = lane >> 4;
+    float cs4[4] = {1.f, 1.f, 1.f, 1.f};   // column scale of target slot 32k + lane
+    if (MODE == 0 && csc)
+#pragma unroll
+        for (int k = 0; k < 4; ++k) cs4[k] = 32 * k + lane < nt ? csc[tgt + 32 * k + lane] : 1.f;
+    // this chain's scale undone on a 16-column chunk starting at column c
+    auto unscale = [&](float (&x)[16], int c) {
+        if (!scaled) return;
+        const int b = c & 127, k = b >> 5;
+        const float src = k == 0 ? cs4[0] : k == 1 ? cs4[1] : k == 2 ? cs4[2] : cs4[3];
+#pragma unroll
+        for (int m = 0; m < 16; ++m) x[m] *= fsc * __shfl_sync(0xffffffffu, src, (b & 31) + m);
+    };
     int idx[4] = {0, 0, 0, 0};   // caller index of target slot 32k + lane
     if (MODE == 0 && end)
 #pragma unroll
@@ -301,6 +376,8 @@ __device__ __noinline__ void fold_chain(uint32_t td, int q, int lane, bool end, 
                 tmem_ld16(td + 256 + c1, r1);
             }
             tmem_wait_ld();
+            unscale(x0, c0);
+            unscale(x1, c1);
             if (!first) {
 #pragma unroll
                 for (int m = 0; m < 16; ++m) {
@@ -321,6 +398,7 @@ __device__ __noinline__ void fold_chain(uint32_t td, int q, int lane, bool end, 
         tmem_ld16(td + c, x);
         if (!first) tmem_ld16(td + 256 + c, r);
         tmem_wait_ld();
+        unscale(x, c);
         if (!first) {
 #pragma unroll
             for (int m = 0; m < 16; ++m) x[m] += r[m];
@@ -334,8 +412,11 @@ __device__ __noinline__ void fold_chain(uint32_t td, int q, int lane, bool end, 
 // JOINT: one launch over the groups of several grids (of one degree): group
 // gi belongs to the grid k with J.beg[k] <= gi < J.beg[k + 1] and carries
 // that grid's arguments.  Otherwise J.g[0] is the only grid.
-template <int MODE, bool JOINT>
+template <int MODE, bool JOINT, bool F16>
 __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(const __grid_constant__ TcJoint J, int *err) {
+    static_assert(!F16 || MODE == 0, "FP16 operands in the leaf pass only");
+    constexpr int SK = F16 ? kStageKF16 : kStageK;   // sources per stage
+    constexpr int SU = SK / 8;                        // store units (8 sources) per stage
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     TcSmem &sm = *reinterpret_cast<TcSmem *>(smem_raw);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -386,14 +467,14 @@ __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(const __grid_const
 
     if (warp < kProdWarps) {
         // ============================================================ producers
-        // A stage's tasks are (row block of 32 targets, k-step) pairs, one
-        // 8-source k-step of 32 rows each.  A stage costs the latency of the
-        // busiest warp's tasks, so the tasks of small groups (one or two
-        // row blocks: the second tile of a leaf with more than 128 points)
-        // are spread over all warps:
-        //   3-4 row blocks: warp w takes row block w % 4, k-steps w / 4, w / 4 + 2
-        //   2 row blocks:   warp w takes row block w % 2, k-step w / 2
-        //   1 row block:    warp w < 4 takes k-step w (warps 4-7 only arrive)
+        // A stage's tasks are (row block of 32 targets, unit) pairs, one
+        // 8-source unit of 32 rows each (a TF32 stage has 4 units, an FP16
+        // stage 8).  A stage costs the latency of the busiest warp's tasks,
+        // so the tasks of small groups (one or two row blocks: the second
+        // tile of a leaf with more than 128 points) are spread over all warps:
+        //   3-4 row blocks: warp w takes row block w % 4, units w / 4 + 2i
+        //   2 row blocks:   warp w takes row block w % 2, units w / 2 + 4i
+        //   1 row block:    warp w takes unit w (TF32: warps 4-7 only arrive)
         // The source coordinates of a stage's k-steps (x[8] y[8] z[8] each,
         // relative to their panel's centre) arrive in shared memory with the
         // stage's weights: the loader warp copies them up to kWStages stages
@@ -407,7 +488,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(const __grid_const
             const int rb = (G.nt + 31) >> 5;
             const int wb = rb >= 3 ? (warp & 3) : rb == 2 ? (warp & 1) : 0;            // row block
             const int kfirst = rb >= 3 ? (warp >> 2) : rb == 2 ? (warp >> 1) : warp;    // first k-step
-            const int kstride = rb >= 3 ? 2 : kStageKs;
+            const int kstride = rb >= 3 ? 2 : rb == 2 ? 4 : 8;
             const int row = 32 * wb + lane;
             const bool active = 32 * wb < G.nt, rvalid = row < G.nt;
             // canonical offsets (floats) of this thread's rows in a kernel tile:
@@ -416,9 +497,14 @@ __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(const __grid_const
             const int on = canon(MODE == 0 ? kTcRows + row : kTcProxyRows + row, 0) >> 2;
             const int oz = canon(MODE == 0 ? 0 : 2 * kTcProxyRows + row, 0) >> 2;
             const bool row_in_tile = MODE != 1 || row < kTcProxyRows;   // proxy components hold 85 rows
+            // FP16 tiles: byte offset of the row's first K core matrix (8-row
+            // groups 256 B apart, the two K halves 128 B apart)
+            const int oe16 = (row >> 3) * 256 + (row & 7) * 16, on16 = oe16 + (kTcRows / 8) * 256;
             // the row's target relative to the leaf centre and its east /
             // north unit vectors (zero at the poles, as the reference's guard)
             float tl0 = 0.f, tl1 = 0.f, tl2 = 0.f, el0 = 0.f, el1 = 0.f, ep0 = 0.f, ep1 = 0.f, ep2 = 0.f;
+            // FP16 leaf pass: this row's power-of-two scale of kernel values
+            const float tsc = (F16 && rvalid) ? a.tscale[G.tgt + row] : 1.f;
             // upward: this row's proxy p = row0 + row = up_i + up_j n
             const int up_p = MODE == 2 ? G.row0 + (rvalid ? row : 0) : 0;
             const int up_i = up_p % n, up_j = up_p / n;
@@ -467,7 +553,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(const __grid_const
                 const TcItem it = nxt;
                 if (k + 1 < ni) nxt = a.items[G.ib + k + 1];
                 const int kind = it.kind & 3;
-                const int nst = (it.cnt + kStageK - 1) / kStageK;
+                const int nst = (it.cnt + SK - 1) / SK;
                 if (MODE == 0 && kind == 2 && it.off != cur_slot) {
                     // BLI bases of every target row in the new slot: thread
                     // t < 128 the xi basis of target t, thread 128 + t its
@@ -489,7 +575,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(const __grid_const
                 const bool self_item = MODE == 0 && kind == 0 && it.off < G.tgt + G.nt && G.tgt < it.off + it.cnt;
                 for (int j = 0; j < nst; ++j, ++st) {
                     const uint32_t slot = st % kKStages, kpar = ((st / kKStages) - 1) & 1;
-                    const int nks = (min(kStageK, it.cnt - kStageK * j) + 7) >> 3;   // k-steps of this stage
+                    const int nks = (min(SK, it.cnt - SK * j) + 7) >> 3;   // k-steps of this stage
                     // the MMAs that last read this slot must be done before
                     // the first store into it
                     bool slot_free = st < (uint32_t)kKStages;
@@ -517,7 +603,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(const __grid_const
                             } else if (MODE == 0 && kind == 2) {
                                 // DOWN: BLI basis of the target x its unit vector's
                                 // component of the Cartesian row
-                                const int *km0 = sm.kmap + it.row0 + kStageK * j + 8 * kk;
+                                const int *km0 = sm.kmap + it.row0 + SK * j + 8 * kk;
                                 const float *fxr = sm.fx[row], *fer = sm.fe[row];
 #pragma unroll
                                 for (int c = 0; c < 8; ++c) {
@@ -573,7 +659,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(const __grid_const
                                 }
                                 // the target itself among these 8 sources: the self pair
                                 if (self_item) {
-                                    const int cs = my_pos - (it.off + kStageK * j + 8 * kk);
+                                    const int cs = my_pos - (it.off + SK * j + 8 * kk);
                                     if ((unsigned)cs < 8u) {
 #pragma unroll
                                         for (int c = 0; c < 8; ++c)
@@ -584,6 +670,27 @@ __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(const __grid_const
                     };
                     // its TF32 hi + lo split, stored into the kernel tile
                     auto store = [&](int kk, const float (&ve)[8], const float (&vn)[8], const float (&vz)[8]) {
+                            if constexpr (F16) {
+                                // FP16 hi + lo: unit kk is K half kk & 1 of MMA step kk / 2,
+                                // the row's 8 values one 16-byte core-matrix row
+                                char *th = reinterpret_cast<char *>(sm.Kt[slot][kk >> 1][0]);
+                                char *tlo = reinterpret_cast<char *>(sm.Kt[slot][kk >> 1][1]);
+                                const int hb = 128 * (kk & 1);
+                                uint4 eh, el, nh, nl;
+                                split_f16x2(ve[0], ve[1], eh.x, el.x);
+                                split_f16x2(ve[2], ve[3], eh.y, el.y);
+                                split_f16x2(ve[4], ve[5], eh.z, el.z);
+                                split_f16x2(ve[6], ve[7], eh.w, el.w);
+                                split_f16x2(vn[0], vn[1], nh.x, nl.x);
+                                split_f16x2(vn[2], vn[3], nh.y, nl.y);
+                                split_f16x2(vn[4], vn[5], nh.z, nl.z);
+                                split_f16x2(vn[6], vn[7], nh.w, nl.w);
+                                *reinterpret_cast<uint4 *>(th + oe16 + hb) = eh;
+                                *reinterpret_cast<uint4 *>(tlo + oe16 + hb) = el;
+                                *reinterpret_cast<uint4 *>(th + on16 + hb) = nh;
+                                *reinterpret_cast<uint4 *>(tlo + on16 + hb) = nl;
+                                return;
+                            }
                             // TF32 hi + lo (the tensor cores read lo's top 11 bits)
                             float *th = sm.Kt[slot][kk][0], *tlo = sm.Kt[slot][kk][1];
 #pragma unroll
@@ -616,10 +723,24 @@ __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(const __grid_const
                                 }
                             }
                     };
+                    // FP16: an odd last unit's partner in its 16-source MMA
+                    // step is written as zeros
+                    const int nut = F16 ? ((nks + 1) & ~1) : nks;
 #pragma unroll 1
-                    for (int kk = kfirst; active && kk < nks; kk += kstride) {
+                    for (int kk = kfirst; active && kk < nut; kk += kstride) {
                         float ve[8], vn[8], vz[8];
-                        values(kk, ve, vn, vz);
+                        if (!F16 || kk < nks) {
+                            values(kk, ve, vn, vz);
+                            if (F16 && kind != 2)
+#pragma unroll
+                                for (int c = 0; c < 8; ++c) {
+                                    ve[c] *= tsc;
+                                    vn[c] *= tsc;
+                                }
+                        } else {
+#pragma unroll
+                            for (int c = 0; c < 8; ++c) ve[c] = vn[c] = vz[c] = 0.f;
+                        }
                         if (!slot_free) {
                             wait_bounded(&sm.kempty[slot], kpar, abort, err);
                             slot_free = true;
@@ -650,7 +771,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(const __grid_const
             for (int k = G.ib; k < G.ie; ++k) {
                 const TcItem it = nxt;
                 if (k + 1 < G.ie) nxt = a.items[k + 1];
-                const int nst = (it.cnt + kStageK - 1) / kStageK;
+                const int nst = (it.cnt + SK - 1) / SK;
                 for (int j = 0; j < nst; ++j, ++st) {
                     const uint32_t slot = st % kKStages, jb = st % kWStages;
                     wait_bounded(&sm.wfull[jb], (st / kWStages) & 1, abort, err);
@@ -661,12 +782,22 @@ __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(const __grid_const
                     tc_fence_after();
                     if (lane == 0) {
                         if (!*abort) {
-                            const int nks = (min(kStageK, it.cnt - kStageK * j) + 7) >> 3;
-                            for (int s = 0; s < nks; ++s) {
-                                const uint64_t aw = smem_desc(&sm.Wt[jb][s * kWStepFloats]);
-                                const uint64_t bh = smem_desc(sm.Kt[slot][s][0]), bl = smem_desc(sm.Kt[slot][s][1]);
-                                mma_ss(tmem, aw, bh, (chain_open || s > 0) ? 1u : 0u);
-                                mma_ss(tmem, aw, bl, 1u);
+                            const int nks = (min(SK, it.cnt - SK * j) + 7) >> 3;
+                            if constexpr (F16) {
+                                // 16 sources per MMA: weight units 2s and 2s + 1
+                                for (int s = 0; 2 * s < nks; ++s) {
+                                    const uint64_t aw = smem_desc_w16(&sm.Wt[jb][s * (2 * kW16UnitBytes / 4)]);
+                                    const uint64_t bh = smem_desc(sm.Kt[slot][s][0]), bl = smem_desc(sm.Kt[slot][s][1]);
+                                    mma_ss_f16(tmem, aw, bh, (chain_open || s > 0) ? 1u : 0u);
+                                    mma_ss_f16(tmem, aw, bl, 1u);
+                                }
+                            } else {
+                                for (int s = 0; s < nks; ++s) {
+                                    const uint64_t aw = smem_desc(&sm.Wt[jb][s * kWStepFloats]);
+                                    const uint64_t bh = smem_desc(sm.Kt[slot][s][0]), bl = smem_desc(sm.Kt[slot][s][1]);
+                                    mma_ss(tmem, aw, bh, (chain_open || s > 0) ? 1u : 0u);
+                                    mma_ss(tmem, aw, bl, 1u);
+                                }
                             }
                         }
                         mma_commit(&sm.kempty[slot]);
@@ -704,17 +835,23 @@ __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(const __grid_const
                     // into L2 while this item's stages run
                     if (lane == 0 && MODE != 2) {
                         const uint32_t nks = (uint32_t)(nxt.cnt + 7) >> 3;
-                        prefetch_l2(a.bstore + (size_t)nxt.kb * kWStepFloats, nks * kWStepFloats * 4u);
+                        if (F16)
+                            prefetch_l2(static_cast<const char *>(a.bstore16) + (size_t)nxt.kb * kW16UnitBytes,
+                                        ((nks + 1) & ~1u) * kW16UnitBytes);
+                        else
+                            prefetch_l2(a.bstore + (size_t)nxt.kb * kWStepFloats, nks * kWStepFloats * 4u);
                         if ((nxt.kind & 3) != 2) prefetch_l2(a.sxyz + (size_t)nxt.kb * 24, nks * 96u);
                     }
                 }
-                const int nst = (it.cnt + kStageK - 1) / kStageK;
+                const int nst = (it.cnt + SK - 1) / SK;
                 for (int j = 0; j < nst; ++j, ++st) {
                     const uint32_t jb = st % kWStages, ub = st / kWStages;
                     if (ub > 0) wait_bounded(&sm.wempty[jb], (ub - 1) & 1, abort, err);
                     if (lane == 0) {
-                        const int ncol = min(kStageK, it.cnt - kStageK * j), nks = (ncol + 7) >> 3;
-                        const uint32_t wbytes = (uint32_t)nks * kWStepFloats * 4;
+                        const int ncol = min(SK, it.cnt - SK * j), nks = (ncol + 7) >> 3;
+                        // FP16: whole 16-source MMA steps (the store has a spare unit at its end)
+                        const uint32_t wbytes = F16 ? (uint32_t)((nks + 1) & ~1) * kW16UnitBytes
+                                                    : (uint32_t)nks * kWStepFloats * 4;
                         // with the weights: the stage's BLI factors (upward) or
                         // its point / proxy sources' coordinates (24 floats per
                         // k-step; DOWN rows need none)
@@ -724,11 +861,14 @@ __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(const __grid_const
                         if (!*abort) {
                             if (lbytes)
                                 dev::bulk_g2s(sm.aux[jb],
-                                              MODE == 2 ? (const void *)(a.basis + (size_t)(it.row0 + kStageKs * j) * 16 * n)
-                                                        : (const void *)(a.sxyz + (size_t)(it.kb + kStageKs * j) * 24),
+                                              MODE == 2 ? (const void *)(a.basis + (size_t)(it.row0 + SU * j) * 16 * n)
+                                                        : (const void *)(a.sxyz + (size_t)(it.kb + SU * j) * 24),
                                               lbytes, &sm.wfull[jb]);
-                            dev::bulk_g2s(sm.Wt[jb], a.bstore + (size_t)(it.kb + kStageKs * j) * kWStepFloats, wbytes,
-                                          &sm.wfull[jb]);
+                            const void *wsrc =
+                                F16 ? static_cast<const void *>(static_cast<const char *>(a.bstore16) +
+                                                                (size_t)(it.kb + SU * j) * kW16UnitBytes)
+                                    : static_cast<const void *>(a.bstore + (size_t)(it.kb + SU * j) * kWStepFloats);
+                            dev::bulk_g2s(sm.Wt[jb], wsrc, wbytes, &sm.wfull[jb]);
                         }
                     }
                     __syncwarp();
@@ -757,11 +897,18 @@ __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(const __grid_const
                 if (!(a.items[k].kind & kTcFlush)) continue;
                 wait_bounded(&sm.accfull, cc & 1, abort, err);
                 tc_fence_after();
+                // FP16: the chain's weight rows are the fields' source weights
+                // (scaled per field) against scaled kernel columns, or their
+                // potentials (scaled per field) against unscaled DOWN columns
+                const bool down_chain = (a.items[k].kind & 3) == 2;
+                const float fsc = F16 ? 1.f / f16_scale(__uint_as_float(a.fmax[(down_chain ? kF : 0) + 16 * q + (lane & 15)]))
+                                      : 1.f;
                 fold_chain<MODE>(tq, q, lane, k == G.ie - 1, first, G.tgt, G.nt,
                                  a.perm, a.out_x, a.out_y, a.ld_out, a.f0, a.nf, *abort != 0,
                                  MODE == 1   ? a.partial + ((size_t)G.out * P + G.row0) * 3 * kF
                                  : MODE == 2 ? a.partial + ((size_t)G.out * P + G.row0) * kF
-                                             : nullptr);
+                                             : nullptr,
+                                 F16, fsc, F16 && !down_chain ? a.tinv : nullptr);
                 tc_fence_before();
                 __syncwarp();
                 if (lane == 0) mbar_arrive(&sm.accfree);
@@ -803,6 +950,107 @@ __global__ void split_store_kernel(const int32_t *__restrict__ bsrc, int64_t nk,
     *reinterpret_cast<float4 *>(base + oh + 32) = make_float4(hi[4], hi[5], hi[6], hi[7]);
     *reinterpret_cast<float4 *>(base + ol) = make_float4(lo[0], lo[1], lo[2], lo[3]);
     *reinterpret_cast<float4 *>(base + ol + 32) = make_float4(lo[4], lo[5], lo[6], lo[7]);
+}
+
+// FP16 leaf pass: per field the largest |value| of the split store's rows
+// (units [0, nu)): source weights into out[f], potentials into out[64 + f],
+// as float bits with atomicMax (non-negative floats order as their bits).
+// Thread t: field t % 64 of units t / 64, t / 64 + stride, ...
+__global__ void field_max_kernel(const int32_t *__restrict__ bsrc, int64_t nu, const float *__restrict__ wF,
+                                 const float *__restrict__ phiF, unsigned *__restrict__ out) {
+    __shared__ float pw[256], pp[256];
+    const int f = threadIdx.x & (kF - 1);
+    float mw = 0.f, mp = 0.f;
+    const int64_t stride = (int64_t)gridDim.x * (blockDim.x / kF);
+    for (int64_t u = (int64_t)blockIdx.x * (blockDim.x / kF) + (threadIdx.x / kF); u < nu; u += stride)
+#pragma unroll
+        for (int r = 0; r < 8; ++r) {
+            const int32_t s = bsrc[u * 8 + r];
+            if (s >= 0) mw = fmaxf(mw, fabsf(wF[(size_t)s * kF + f]));
+            else if (s <= -2) mp = fmaxf(mp, fabsf(phiF[(size_t)(-2 - s) * kF + f]));
+        }
+    pw[threadIdx.x] = mw;
+    pp[threadIdx.x] = mp;
+    __syncthreads();
+    if (threadIdx.x < kF) {
+        for (int i = kF + threadIdx.x; i < (int)blockDim.x; i += kF) {
+            mw = fmaxf(mw, pw[i]);
+            mp = fmaxf(mp, pp[i]);
+        }
+        atomicMax(out + f, __float_as_uint(mw));
+        atomicMax(out + kF + f, __float_as_uint(mp));
+    }
+}
+
+// FP16 hi/lo weight store: per unit of 8 store rows, the 64-field rows as
+// one 128-row FP16 tile (field f's hi part at row wrow(f, 0), lo at
+// wrow(f, 1); row m at byte (m / 8) 128 + (m % 8) 16, 8 halves), source
+// weights scaled by their field's power of two, potentials by theirs.  One
+// thread per (unit, field).
+__global__ void split_store16_kernel(const int32_t *__restrict__ bsrc, int64_t nu, const float *__restrict__ wF,
+                                     const float *__restrict__ phiF, const unsigned *__restrict__ fmax,
+                                     unsigned char *__restrict__ out) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nu * kF) return;
+    const int64_t u = t / kF;
+    const int f = (int)(t % kF);
+    const float sw = f16_scale(__uint_as_float(fmax[f])), sp = f16_scale(__uint_as_float(fmax[kF + f]));
+    float v[8];
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+        const int32_t s = bsrc[u * 8 + r];
+        v[r] = s >= 0 ? wF[(size_t)s * kF + f] * sw : (s <= -2 ? phiF[(size_t)(-2 - s) * kF + f] * sp : 0.f);
+    }
+    uint4 hi, lo;
+    split_f16x2(v[0], v[1], hi.x, lo.x);
+    split_f16x2(v[2], v[3], hi.y, lo.y);
+    split_f16x2(v[4], v[5], hi.z, lo.z);
+    split_f16x2(v[6], v[7], hi.w, lo.w);
+    unsigned char *base = out + u * kW16UnitBytes;
+    const int mh = wrow(f, 0), ml = wrow(f, 1);
+    *reinterpret_cast<uint4 *>(base + (mh >> 3) * 128 + (mh & 7) * 16) = hi;
+    *reinterpret_cast<uint4 *>(base + (ml >> 3) * 128 + (ml & 7) * 16) = lo;
+}
+
+// FP16 leaf pass: per target the power of two that takes its largest kernel
+// value (east or north, over its PP and PC sources, with the leaf pass's own
+// FP32 arithmetic, and its self pair) to at most 2^12, and the inverse.  One
+// block per leaf group, thread t its target t.  Once per plan.
+__global__ void target_scales_kernel(const TcArgs a, float *__restrict__ tscale, float *__restrict__ tinv) {
+    const MixGroup G = a.groups[blockIdx.x];
+    const int row = threadIdx.x;
+    if (row >= G.nt) return;
+    const double4 c = a.tgt[G.tgt + row];
+    const float tl0 = (float)(c.x - G.cx), tl1 = (float)(c.y - G.cy), tl2 = (float)(c.z - G.cz);
+    float el0 = 0.f, el1 = 0.f, ep0 = 0.f, ep1 = 0.f, ep2 = 0.f;
+    if ((fabs(c.z - 1.0) > 1e-15) && (fabs(c.z + 1.0) > 1e-15)) {
+        const double omz = 1.0 - c.z * c.z, inv = 1.0 / sqrt(omz);
+        el0 = (float)(-c.y * inv);
+        el1 = (float)(c.x * inv);
+        ep0 = (float)(-c.z * c.x * inv);
+        ep1 = (float)(-c.z * c.y * inv);
+        ep2 = (float)(omz * inv);
+    }
+    const double2 sk = a.selfk[G.tgt + row];
+    float m = fmaxf(fabsf((float)sk.x), fabsf((float)sk.y));
+    for (int k = G.ib; k < G.ie; ++k) {
+        const TcItem it = a.items[k];
+        if ((it.kind & 3) == 2) continue;
+        const float tx = tl0 - it.dx, ty = tl1 - it.dy, tz = tl2 - it.dz;
+        for (int i = 0; i < it.cnt; ++i) {
+            const float *u = a.sxyz + (size_t)(it.kb + (i >> 3)) * 24;
+            const float dx = u[i & 7] - tx, dy = u[8 + (i & 7)] - ty, dz = u[16 + (i & 7)] - tz;
+            const float mp = fmaxf(dz * dz + (dy * dy + dx * dx), 1e-20f);
+            const float r = rsqrt_approx(mp);
+            const float uu = rcp_approx(mp * r + 2.f);
+            const float v = (kC1F * r + (kTwoC2F * uu - kTwoC2F)) * (r * r);
+            const float pe = el0 * dx + el1 * dy, pn = ep0 * dx + ep1 * dy + ep2 * dz;
+            m = fmaxf(m, fmaxf(fabsf(v * pe), fabsf(v * pn)));
+        }
+    }
+    const float sc = f16_scale(m);
+    tscale[G.tgt + row] = sc;
+    tinv[G.tgt + row] = 1.f / sc;
 }
 
 // Per pool row, the FP32 coordinates relative to the centre of the row's own
@@ -880,30 +1128,30 @@ size_t tc_smem_bytes() {
     return need > 120 * 1024 ? need : 120 * 1024;
 }
 
-template <int MODE, bool JOINT>
+template <int MODE, bool JOINT, bool F16 = false>
 static void launch_tc(const TcJoint &J, int nsm, int cta_groups, int *err, cudaStream_t st) {
     const int total = J.beg[J.ngrids];
     if (total <= 0) return;
     const size_t smem = tc_smem_bytes();
     static std::atomic<unsigned long long> done{0};
-    smem_attr_once((const void *)tc_leaf_kernel<MODE, JOINT>, (int)smem, done);
+    smem_attr_once((const void *)tc_leaf_kernel<MODE, JOINT, F16>, (int)smem, done);
     // every SM busy, but no CTA longer than cta_groups groups: with short
     // CTAs, kernels of other streams (higher-priority grids) get SMs as CTAs
     // retire
     const int per = cta_groups > 0 ? cta_groups : 1;
     int grid = (total + per - 1) / per;
     if (grid < nsm) grid = total < nsm ? total : nsm;
-    tc_leaf_kernel<MODE, JOINT><<<grid, kThreads, smem, st>>>(J, err);
+    tc_leaf_kernel<MODE, JOINT, F16><<<grid, kThreads, smem, st>>>(J, err);
 }
 
-template <int MODE>
+template <int MODE, bool F16 = false>
 static void launch_tc(const TcArgs &a, int nsm, int cta_groups, int *err, cudaStream_t st) {
     TcJoint J{};
     J.g[0] = a;
     J.ngrids = 1;
     J.beg[0] = 0;
     J.beg[1] = a.ngroups;
-    launch_tc<MODE, false>(J, nsm, cta_groups, err, st);
+    launch_tc<MODE, false, F16>(J, nsm, cta_groups, err, st);
 }
 
 void launch_tc_leaf_joint(const TcArgs *grids, int ngrids, int nsm, int cta_groups, int *err, cudaStream_t st) {
@@ -914,10 +1162,19 @@ void launch_tc_leaf_joint(const TcArgs *grids, int ngrids, int nsm, int cta_grou
         J.g[k] = grids[k];
         J.beg[k + 1] = J.beg[k] + grids[k].ngroups;
     }
-    launch_tc<0, true>(J, nsm, cta_groups, err, st);
+    // the caller checks that all grids use one operand precision
+    if (grids[0].bstore16)
+        launch_tc<0, true, true>(J, nsm, cta_groups, err, st);
+    else
+        launch_tc<0, true, false>(J, nsm, cta_groups, err, st);
 }
 
-void launch_tc_leaf(const TcArgs &a, int nsm, int cg, int *err, cudaStream_t st) { launch_tc<0>(a, nsm, cg, err, st); }
+void launch_tc_leaf(const TcArgs &a, int nsm, int cg, int *err, cudaStream_t st) {
+    if (a.bstore16)
+        launch_tc<0, true>(a, nsm, cg, err, st);
+    else
+        launch_tc<0, false>(a, nsm, cg, err, st);
+}
 void launch_tc_proxy(const TcArgs &a, int nsm, int cg, int *err, cudaStream_t st) { launch_tc<1>(a, nsm, cg, err, st); }
 void launch_tc_upward(const TcArgs &a, int nsm, int cg, int *err, cudaStream_t st) { launch_tc<2>(a, nsm, cg, err, st); }
 
@@ -928,6 +1185,25 @@ void launch_split_store(const int32_t *bsrc, int64_t k0, int64_t k1, const float
     const int64_t threads = nk * kF;
     split_store_kernel<<<(unsigned)((threads + 255) / 256), 256, 0, st>>>(bsrc + k0 * 8, nk, wF, phiF,
                                                                           bstore + k0 * kWStepFloats);
+}
+
+void launch_field_max(const int32_t *bsrc, int64_t nunits, const float *wF, const float *phiF, unsigned *fmax,
+                      cudaStream_t st) {
+    if (nunits > 0)
+        field_max_kernel<<<(unsigned)std::min<int64_t>((nunits + 3) / 4, 148 * 16), 256, 0, st>>>(bsrc, nunits, wF,
+                                                                                                   phiF, fmax);
+}
+
+void launch_split_store16(const int32_t *bsrc, int64_t nunits, const float *wF, const float *phiF,
+                          const unsigned *fmax, void *bstore16, cudaStream_t st) {
+    if (nunits <= 0) return;
+    const int64_t threads = nunits * kF;
+    split_store16_kernel<<<(unsigned)((threads + 255) / 256), 256, 0, st>>>(bsrc, nunits, wF, phiF, fmax,
+                                                                            static_cast<unsigned char *>(bstore16));
+}
+
+void launch_target_scales(const TcArgs &a, float *tscale, float *tinv, cudaStream_t st) {
+    if (a.ngroups > 0) target_scales_kernel<<<a.ngroups, kTcRows, 0, st>>>(a, tscale, tinv);
 }
 
 void launch_source_local(const double4 *pool, const int2 *ranges, const double4 *centres, int nranges, float4 *sloc,

@@ -78,6 +78,7 @@ class Tune(C.Structure):
     _fields_ = [
         ("chain_ksteps", C.c_int32), ("tree_passes", C.c_int32), ("up_chunk", C.c_int32),
         ("proxy_unit_kpairs", C.c_int32), ("cta_groups", C.c_int32), ("field_block", C.c_int32),
+        ("f16", C.c_int32),
     ]
 
     def as_dict(self):

@@ -21,12 +21,16 @@ def _torch():
     return torch
 
 
-def _grid(name, thresh, nfields, seed=11, degree=8):
+def _grid(name, thresh, nfields, seed=11, degree=8, max_fields=None):
+    """A grid and nfields seeded fields.  max_fields > 32 gives 64-field blocks
+    (the tcgen05 passes) whatever nfields is; the default sizes the blocks for
+    nfields (32-field mma.sync blocks below 33)."""
     import salgpu as S
     g, hs = grid_and_ssh(name, nfields=nfields, seed=seed)
     t = S.tree_traverse(g.xs, g.ys, g.zs, g.n, thresh)
     L = S.dual_tree_traversal(t, 0.7, thresh)
-    return S, g, hs, S.Grid(t, g.xs, g.ys, g.zs, g.areas, degree, S.MODE_DTT, L, max_fields=nfields)
+    mf = nfields if max_fields is None else max_fields
+    return S, g, hs, S.Grid(t, g.xs, g.ys, g.zs, g.areas, degree, S.MODE_DTT, L, max_fields=mf)
 
 
 @pytest.mark.parametrize("name,thresh", [("small_3000", 20), ("cfg0", 100)])
@@ -167,9 +171,9 @@ def test_tree_passes_match_direct_passes(degree):
     the bars against the FP64 accurate form and the direct sum.  The basis
     work they report falls."""
     torch = _torch()
-    S, g, hs, grid = _grid("small_20000", 60, 4, seed=2, degree=degree)
+    S, g, hs, grid = _grid("small_20000", 60, 4, seed=2, degree=degree, max_fields=64)
     ssh = torch.tensor(hs, device="cuda")
-    assert grid.tune()["tree_passes"] == 1
+    assert grid.tune()["tree_passes"] == 1 and grid.tune()["field_block"] == 64
     tx, ty = grid.solve(ssh, form=S.FORM_MIXED)
     st_tree = grid.stats()
     grid.tune(tree_passes=0)
@@ -196,11 +200,12 @@ def test_tune_settings_round_trip_and_keep_accuracy():
     shape) and the batched form stays within its bar of the FP64 accurate
     form; bad settings are refused."""
     torch = _torch()
-    S, g, hs, grid = _grid("small_20000", 60, 3, seed=8)
+    S, g, hs, grid = _grid("small_20000", 60, 3, seed=8, max_fields=64)
     ssh = torch.tensor(hs, device="cuda")
     ax, ay = grid.solve(ssh, form=S.FORM_ACCURATE)
     settings = [dict(chain_ksteps=8), dict(chain_ksteps=64), dict(cta_groups=3), dict(proxy_unit_kpairs=100),
-                dict(tree_passes=0, up_chunk=1000), dict(field_block=32), dict(field_block=64, tree_passes=1)]
+                dict(tree_passes=0, up_chunk=1000), dict(f16=1), dict(tree_passes=1), dict(f16=0),
+                dict(field_block=32), dict(field_block=64, tree_passes=1)]
     for ch in settings:
         now = grid.tune(**ch)
         for k, v in ch.items():
@@ -219,7 +224,7 @@ def test_tune_settings_round_trip_and_keep_accuracy():
 
 def test_autotune_picks_a_setting_within_the_bar():
     torch = _torch()
-    S, g, hs, grid = _grid("small_20000", 60, 4, seed=12)
+    S, g, hs, grid = _grid("small_20000", 60, 4, seed=12, max_fields=64)
     ssh = torch.tensor(hs, device="cuda")
     best, ms_best, ms_start = grid.autotune(ssh, ntargets=1000, max_rel_err=5e-6)
     assert grid.tune() == best
@@ -278,3 +283,56 @@ def test_mixed_bytes_estimate_equals_the_allocation(nfields):
     st = grid.stats()
     assert st["mixed_bytes"] == est
     assert st["device_bytes"] - before == est
+
+
+@pytest.mark.parametrize("degree,tree", [(8, 1), (10, 1), (8, 0)])
+def test_f16_leaf_pass_matches_tf32_and_direct_sum(degree, tree):
+    """The FP16 leaf pass (sal_tune.f16 = 1: kind::f16 MMAs of 16 sources,
+    FP16 hi + lo operands scaled by powers of two per target and per field)
+    against the TF32 leaf pass and the FP64 accurate form (5e-6) and the FP64
+    direct sum (1e-5), with the tree passes and with the direct passes (DOWN
+    items between the kernel items), on fields of very different amplitude
+    (the per-field scales must keep small fields as accurate as large ones)."""
+    torch = _torch()
+    S, g, hs, grid = _grid("small_20000", 60, 6, seed=5, degree=degree, max_fields=64)
+    hs = hs * np.array([1.0, 1e-3, 1e3, 1e-6, 1.0, 5.0])[:, None]
+    ssh = torch.tensor(hs, device="cuda")
+    grid.tune(tree_passes=tree, f16=0)
+    tx, ty = grid.solve(ssh, form=S.FORM_MIXED)
+    grid.tune(f16=1)
+    assert grid.tune()["f16"] == 1
+    fx, fy = grid.solve(ssh, form=S.FORM_MIXED)
+    ax, ay = grid.solve(ssh, form=S.FORM_ACCURATE)
+    torch.cuda.synchronize()
+    grid.sync()
+    T = lambda a: torch.tensor(a, device="cuda")
+    tg = np.sort(np.random.default_rng(6).choice(g.n, 3000, replace=False)).astype(np.int32)
+    for f in range(6):
+        t = [v[f].cpu().numpy() for v in (fx, fy, tx, ty, ax, ay)]
+        assert np.all(np.isfinite(t[0])) and np.all(np.isfinite(t[1]))
+        assert rel_l2(t[0], t[1], t[2], t[3]) <= 5e-6
+        assert rel_l2(t[0], t[1], t[4], t[5]) <= 5e-6
+        rx, ry = S.direct_sum(T(g.xs), T(g.ys), T(g.zs), T(g.areas * hs[f]), T(tg))
+        assert rel_l2(t[0][tg], t[1][tg], rx.cpu().numpy(), ry.cpu().numpy()) <= 1e-5
+
+
+def test_f16_joint_solve_equals_separate_solves_and_memory_estimate():
+    """FP16 leaf passes of two grids in one launch equal their separate
+    solves bit for bit; the batched-memory estimate counts the FP16 buffers."""
+    torch = _torch()
+    grids, sshs = [], []
+    for name, thresh in (("small_3000", 20), ("cfg0", 100)):
+        S, g, hs, grid = _grid(name, thresh, 5, seed=9, max_fields=64)
+        grid.tune(f16=1)
+        est = grid.stats()["mixed_bytes"]
+        before = grid.stats()["device_bytes"]
+        grids.append(grid)
+        sshs.append(torch.tensor(hs, device="cuda"))
+        sep = grid.solve(sshs[-1], form=S.FORM_MIXED)
+        torch.cuda.synchronize()
+        assert grid.stats()["device_bytes"] - before == est
+        grid.sep = [v.clone() for v in sep]
+    outs = S.solve_joint(grids, sshs)
+    torch.cuda.synchronize()
+    for grid, (ox, oy) in zip(grids, outs):
+        assert torch.equal(ox, grid.sep[0]) and torch.equal(oy, grid.sep[1])
