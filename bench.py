@@ -177,8 +177,8 @@ def cpu_baseline(args, g, h, sample_seconds):
 
 def workload_name(args, n):
     form = {"ref": "plain FP64 (reference operation order)", "accurate": "FP64 accurate form",
-            "mixed": "batched mixed precision: FP32 kernel tiles, TF32 hi/lo tensor-core contractions "
-                     "(tcgen05 leaf pass), FP64 self pairs"}[args.form]
+            "mixed": "batched mixed precision: FP32 kernel tiles, TF32 or (autotuner's choice) scaled FP16 hi/lo "
+                     "tensor-core contractions (tcgen05), FP64 self pairs"}[args.form]
     return (f"{args.config}: {n} cells x {args.fields} SSH fields, dual tree traversal (code.f90 fast_sum), "
             f"d={args.degree}, theta={args.theta}, leaf<{args.thresh}; {form}")
 
@@ -629,19 +629,23 @@ def main():
         except (OSError, ValueError):
             pass
         bf16 = peaks.get("bf16_tflops", 1590.0)
-        peak = bf16 / 2.0          # dense TF32 = half the bf16 rate
+        f16 = F == 64 and grid.tune().get("f16", 0) == 1
+        # the leaf pass's MMAs: kind::f16 (dense FP16 = the bf16 rate) or kind::tf32 (half of it)
+        peak = bf16 if f16 else bf16 / 2.0
         leaf_flops = 4.0 * F * (st["pairs_pp"] + st["pairs_pc"] + 3.0 * st["macs_down_batched"])
         achieved = leaf_flops / (leaf_ms * 1e-3) / 1e12
-        roof = {"bound": "tensor", "kernel": "tc_leaf_kernel<0> (tcgen05 TF32 hi/lo, M=128 field parts x N=256 target "
-                          "components; PP+PC kernel tiles, DOWN interpolation) + split_store_kernel (potentials)",
+        prec = "FP16" if f16 else "TF32"
+        src = "bf16_tflops of measured" if "bf16_tflops" in peaks else "1.59 PFLOP/s bf16 fallback"
+        roof = {"bound": "tensor", "kernel": f"tc_leaf_kernel<0> (tcgen05 {prec} hi/lo, M=128 field parts x N=256 "
+                          "target components; PP+PC kernel tiles, DOWN interpolation) + its weight store",
                 "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-                "peak_source": ("TF32 dense = bf16_tflops/2 of measured" if "bf16_tflops" in peaks else
-                                "TF32 dense = 1.59 PFLOP/s bf16 fallback / 2"),
+                "peak_source": (f"FP16 dense = {src}" if f16 else f"TF32 dense = {src} / 2"),
                 "flops_counted": "algorithmic 4*F per pair (2 components x FMA x F fields); the hi/lo split "
                                  "executes 4x these on the tensor cores (W_hi,W_lo x T_hi,T_lo), plus padding",
                 # ncu dram__bytes_read.sum + dram__bytes_write.sum of one tc_leaf_kernel launch on the
-                # 655,362-cell, 64-field case (3.95 + 2.65 GB), scaled by the cell count
-                "traffic": 6.600e9 * g.n / 655362 if F == 64 else None,
+                # 655,362-cell, 64-field case (FP16: 3.14 + 2.61 GB; TF32: 3.95 + 2.65 GB), scaled by the
+                # cell count
+                "traffic": (5.750e9 if f16 else 6.600e9) * g.n / 655362 if F == 64 else None,
                 "traffic_source": "ncu capture on 655,362 cells x 64 fields, scaled by cells",
                 "leaf_ms": leaf_ms, "proxy_ms": proxy_ms, "prep_upward_ms": up_ms}
     else:
@@ -670,7 +674,9 @@ def main():
         line = {
             "metric": METRIC, "value": value, "unit": "evals/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32/tf32 (fp64 self pairs)" if form == S.FORM_MIXED else "f64",
+            "scaling": "weak", "vs_baseline": None, "dtype": (("f32/f16 hi-lo" if grid.tune().get("f16", 0) == 1 else "f32/tf32 hi-lo") + " (fp64 self pairs)"
+                      if form == S.FORM_MIXED and F == 64 else "f32/tf32 (fp64 self pairs)" if form == S.FORM_MIXED
+                      else "f64"),
             "data": "synthetic: seeded Fibonacci ocean grid + spherical-harmonic SSH (stand-in for the MPAS CSVs)",
             "config": {"workload": workload_name(args, g.n), "cells": g.n, "fields": F, "form": args.form,
                        "parallelism": f"replicas x{world}", "l2": "flushed (256 MB write) between timed solves"},

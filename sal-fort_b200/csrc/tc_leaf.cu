@@ -210,11 +210,16 @@ __device__ __forceinline__ uint64_t smem_desc_w16(const void *p) {
     return ((addr >> 4) & 0x3FFFull) | ((uint64_t)(kW16UnitBytes >> 4) << 16) | ((uint64_t)(128 >> 4) << 32) |
            (1ull << 46);
 }
-// FP16 hi + lo of two values, packed as half2 words: hi = round(v), lo = round(v - hi)
+// FP16 hi + lo of two values, packed as half2 words: hi = v rounded to 11
+// significant bits (TF32 rounding; exact in FP16 inside its normal range),
+// lo = v - hi rounded to FP16.
 __device__ __forceinline__ void split_f16x2(float a, float b, uint32_t &hi, uint32_t &lo) {
-    const __half2 h = __floats2half2_rn(a, b);
-    const float2 back = __half22float2(h);
-    const __half2 l = __floats2half2_rn(a - back.x, b - back.y);
+    uint32_t ha, hb;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(ha) : "f"(a));
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(hb) : "f"(b));
+    const float2 r = sub2(make_float2(a, b), make_float2(__uint_as_float(ha), __uint_as_float(hb)));
+    const __half2 h = __floats2half2_rn(__uint_as_float(ha), __uint_as_float(hb));
+    const __half2 l = __floats2half2_rn(r.x, r.y);
     hi = *reinterpret_cast<const uint32_t *>(&h);
     lo = *reinterpret_cast<const uint32_t *>(&l);
 }
@@ -536,15 +541,17 @@ __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(const __grid_const
                 }
                 continue;
             }
-            const float2 el0v = f2(el0), el1v = f2(el1), ep0v = f2(ep0), ep1v = f2(ep1), ep2v = f2(ep2);
+            // the kernel values' projections; FP16: with the row's scale in them
+            const float2 el0v = f2(el0 * tsc), el1v = f2(el1 * tsc), ep0v = f2(ep0 * tsc), ep1v = f2(ep1 * tsc),
+                         ep2v = f2(ep2 * tsc);
             int cur_slot = -1;
             // the self pair (FP64 value / kernel constant, the weight carries the constant)
             const int my_pos = G.tgt + row;
             float self_e = 0.f, self_n = 0.f;
             if (MODE == 0 && rvalid) {
                 const double2 sk = a.selfk[my_pos];
-                self_e = (float)sk.x;
-                self_n = (float)sk.y;
+                self_e = (float)sk.x * tsc;
+                self_n = (float)sk.y * tsc;
             }
             // item records are read one item ahead, so their latency hides
             // behind the current item's stages
@@ -628,11 +635,10 @@ __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(const __grid_const
                                     const float2 dx = sub2((c2 & 1) ? make_float2(X.z, X.w) : make_float2(X.x, X.y), tx2);
                                     const float2 dy = sub2((c2 & 1) ? make_float2(Y.z, Y.w) : make_float2(Y.x, Y.y), ty2);
                                     const float2 dz = sub2((c2 & 1) ? make_float2(Z.z, Z.w) : make_float2(Z.x, Z.y), tz2);
-                                    float2 mp = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
-                                    // mp = 0 only for a source on the target itself (or a
-                                    // repeated point): the clamp keeps the value finite
-                                    mp.x = fmaxf(mp.x, 1e-20f);
-                                    mp.y = fmaxf(mp.y, 1e-20f);
+                                    // + 1e-20: mp = 0 only for a source on the target itself (or
+                                    // a repeated point), and the floor keeps the value finite;
+                                    // chords of neighbours (mp >= 1e-12) do not see it
+                                    const float2 mp = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __ffma2_rn(dx, dx, f2(1e-20f))));
                                     const float2 r = make_float2(rsqrt_approx(mp.x), rsqrt_approx(mp.y));
                                     const float2 w = __fadd2_rn(__fmul2_rn(mp, r), f2(2.f));
                                     const float2 u = make_float2(rcp_approx(w.x), rcp_approx(w.y));
@@ -730,13 +736,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(const __grid_const
                     for (int kk = kfirst; active && kk < nut; kk += kstride) {
                         float ve[8], vn[8], vz[8];
                         if (!F16 || kk < nks) {
-                            values(kk, ve, vn, vz);
-                            if (F16 && kind != 2)
-#pragma unroll
-                                for (int c = 0; c < 8; ++c) {
-                                    ve[c] *= tsc;
-                                    vn[c] *= tsc;
-                                }
+                            values(kk, ve, vn, vz);   // FP16: kernel values come scaled
                         } else {
 #pragma unroll
                             for (int c = 0; c < 8; ++c) ve[c] = vn[c] = vz[c] = 0.f;
