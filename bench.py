@@ -531,6 +531,8 @@ def main():
         best, ms_best, ms_default = grid.autotune(ssh[:64], ntargets=2000, max_rel_err=5e-6)
         tuned = {"default": default, "chosen": best, "ms_default": ms_default, "ms_chosen": ms_best,
                  "search_s": time.perf_counter() - t0}
+    # the leaf pass's operand precision (the autotuner's choice for 64-field blocks)
+    leaf_f16 = form == S.FORM_MIXED and F == 64 and grid.tune().get("f16", 0) == 1
     for _ in range(args.warmup):
         grid.solve(ssh, form=form, out=(ox, oy))
     torch.cuda.synchronize()
@@ -629,7 +631,7 @@ def main():
         except (OSError, ValueError):
             pass
         bf16 = peaks.get("bf16_tflops", 1590.0)
-        f16 = F == 64 and grid.tune().get("f16", 0) == 1
+        f16 = leaf_f16
         # the leaf pass's MMAs: kind::f16 (dense FP16 = the bf16 rate) or kind::tf32 (half of it)
         peak = bf16 if f16 else bf16 / 2.0
         leaf_flops = 4.0 * F * (st["pairs_pp"] + st["pairs_pc"] + 3.0 * st["macs_down_batched"])
@@ -674,7 +676,7 @@ def main():
         line = {
             "metric": METRIC, "value": value, "unit": "evals/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": (("f32/f16 hi-lo" if grid.tune().get("f16", 0) == 1 else "f32/tf32 hi-lo") + " (fp64 self pairs)"
+            "scaling": "weak", "vs_baseline": None, "dtype": (("f32/f16 hi-lo" if leaf_f16 else "f32/tf32 hi-lo") + " (fp64 self pairs)"
                       if form == S.FORM_MIXED and F == 64 else "f32/tf32 (fp64 self pairs)" if form == S.FORM_MIXED
                       else "f64"),
             "data": "synthetic: seeded Fibonacci ocean grid + spherical-harmonic SSH (stand-in for the MPAS CSVs)",

@@ -94,7 +94,9 @@ int sal_dual_tree_traversal(const sal_tree *t, double theta, int32_t cluster_thr
  * per-point (xi, eta) and the panel radii and centres are computed with the
  * host's libm, and MAC ratios within 1e-12 of theta are decided on the host.
  * sal_dual_tree_traversal_device takes any tree (host- or device-built).  Both
- * are synchronous and allocate their device scratch per call. */
+ * are synchronous.  Their device scratch comes from a memory pool of the
+ * library's own per device, which keeps up to 1 GiB between calls (a few
+ * hundred MB after a 2.3M-cell build) until the process exits. */
 int sal_tree_traverse_device(const double *xs, const double *ys, const double *zs, int32_t point_count,
                              int32_t cluster_thresh, int32_t device, sal_tree **out);
 int sal_dual_tree_traversal_device(const sal_tree *t, double theta, int32_t cluster_thresh, int32_t device,
