@@ -175,7 +175,9 @@ int sal_grid_tune_set(sal_grid *g, const sal_tune *t);
  * SAL_FORM_MIXED solves of the caller's nfields device fields (column f at
  * ssh + f * ld_ssh, caller's order, nfields <= 64) for candidate sal_tune
  * settings, by coordinate descent from the current setting over each
- * choice's candidates, with CUDA events on the grid's stream and a 256 MB
+ * choice's candidates (the leaf pass's chain length, operand precision and
+ * groups per CTA a second time at the end), with CUDA events on the grid's
+ * stream and a 256 MB
  * L2 flush before each timed solve.  A candidate counts only if the
  * relative L2 error of its first field, at ntargets evenly spaced points,
  * against the FP64 direct sum stays <= max_rel_err.  The fastest is set on

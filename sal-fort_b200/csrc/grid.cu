@@ -590,6 +590,10 @@ static int ensure_mixed(GridImpl &g, int FT) {
             if (!rc) rc = malloc_mix(g, &g.tscale, n);
             if (!rc) rc = malloc_mix(g, &g.tinv, n);
             if (!rc) {
+                // zeros in every row no pass writes, so the per-field maxima can
+                // read the weight and potential rows whole
+                CK(cudaMemsetAsync(g.wF, 0, (n + (size_t)pl.n_wslots * P) * FT * sizeof(float), g.stream));
+                CK(cudaMemsetAsync(g.phiF, 0, (size_t)pl.n_dslots * 3 * P * FT * sizeof(float), g.stream));
                 CK(cudaMemsetAsync(g.bstore16, 0, units * 2048, g.stream));
                 mix::TcArgs t = leaf_args(g, nullptr, nullptr, 0, 0, 0);
                 mix::launch_target_scales(t, g.tscale, g.tinv, g.stream);
@@ -733,8 +737,9 @@ static void solve_mixed_block(GridImpl &g, const double *ssh, int64_t ld_ssh, in
     // proxies' rows are in place), or FP16 (every row, scaled per field)
     auto leaf_store = [&]() {
         if (g.bstore16) {
+            const size_t nw = (size_t)n + (size_t)pl.n_wslots * P, np = (size_t)pl.n_dslots * 3 * P;
             cudaMemsetAsync(g.fmax, 0, 128 * sizeof(unsigned), st);
-            mix::launch_field_max(g.bsrc, (int64_t)pl.bsrc.size() / 8, g.wF, g.phiF, g.fmax, st);
+            mix::launch_field_max(g.wF, (int64_t)nw, g.phiF, (int64_t)np, g.fmax, st);
             mix::launch_split_store16(g.bsrc, (int64_t)pl.bsrc.size() / 8, g.wF, g.phiF, g.fmax, g.bstore16, st);
         } else {
             mix::launch_split_store(g.bsrc, pl.tc_src_ksteps, (int64_t)pl.bsrc.size() / 8, g.wF, g.phiF, g.bstore, st);
@@ -1074,16 +1079,20 @@ extern "C" int sal_grid_autotune(sal_grid *G, const double *ssh, int32_t nf, int
     const bool start_ok = top_err <= max_rel_err;
     if (!start_ok) top_ms = 1e30;   // any passing setting beats a failing start
     // coordinate descent: each choice's candidates with the others held at
-    // the best so far
+    // the best so far; the leaf pass's choices (chain length, operand
+    // precision, groups per CTA) interact, so they are swept again at the end
     struct Axis { int32_t sal_tune::*field; std::vector<int32_t> values; };
     const std::vector<Axis> axes = {
         {&sal_tune::tree_passes, {1, 0}},
-        {&sal_tune::f16, {0, 1}},
         {&sal_tune::chain_ksteps, {8, 16, 32, 64}},
+        {&sal_tune::f16, {0, 1}},
         {&sal_tune::cta_groups, {1, 2, 4}},
         {&sal_tune::proxy_unit_kpairs, {324, 648, 1296}},
         {&sal_tune::up_chunk, {2048, 4096, 8192}},
         {&sal_tune::field_block, {64, 32}},
+        {&sal_tune::chain_ksteps, {32, 64}},
+        {&sal_tune::f16, {0, 1}},
+        {&sal_tune::cta_groups, {1, 2, 4}},
     };
     for (const Axis &ax : axes) {
         if (ax.field == &sal_tune::up_chunk && top.tree_passes) continue;   // only the direct upward pass uses it

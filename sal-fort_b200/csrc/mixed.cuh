@@ -92,13 +92,12 @@ void launch_basis_store(const int32_t *bas, int64_t nbk, const double2 *xieta, c
 size_t tc_smem_bytes();
 void launch_split_store(const int32_t *bsrc, int64_t k0, int64_t k1, const float *wF, const float *phiF,
                         float *bstore, cudaStream_t st);
-// FP16 leaf pass: per field the largest |value| of the split store's source
-// weight rows and potential rows (units [0, nunits)) into fmax[f] and
-// fmax[64 + f] (float bits; fmax zeroed first); the FP16 hi/lo store of
-// those units with those scales; per target the scale of its kernel values
-// (once per plan).
-void launch_field_max(const int32_t *bsrc, int64_t nunits, const float *wF, const float *phiF, unsigned *fmax,
-                      cudaStream_t st);
+// FP16 leaf pass: per field the largest |value| of the source weight rows
+// (wF, nw rows) and of the potential rows (phiF, np rows) into fmax[f] and
+// fmax[64 + f] (float bits; fmax zeroed first; rows no pass writes must hold
+// zeros); the FP16 hi/lo store of units [0, nunits) with those scales; per
+// target the scale of its kernel values (once per plan).
+void launch_field_max(const float *wF, int64_t nw, const float *phiF, int64_t np, unsigned *fmax, cudaStream_t st);
 void launch_split_store16(const int32_t *bsrc, int64_t nunits, const float *wF, const float *phiF,
                           const unsigned *fmax, void *bstore16, cudaStream_t st);
 void launch_target_scales(const TcArgs &a, float *tscale, float *tinv, cudaStream_t st);
