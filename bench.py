@@ -533,6 +533,7 @@ def main():
                  "search_s": time.perf_counter() - t0}
     # the leaf pass's operand precision (the autotuner's choice for 64-field blocks)
     leaf_f16 = form == S.FORM_MIXED and F == 64 and grid.tune().get("f16", 0) == 1
+    st_after = grid.stats()
     for _ in range(args.warmup):
         grid.solve(ssh, form=form, out=(ox, oy))
     torch.cuda.synchronize()
@@ -645,9 +646,9 @@ def main():
                 "flops_counted": "algorithmic 4*F per pair (2 components x FMA x F fields); the hi/lo split "
                                  "executes 4x these on the tensor cores (W_hi,W_lo x T_hi,T_lo), plus padding",
                 # ncu dram__bytes_read.sum + dram__bytes_write.sum of one tc_leaf_kernel launch on the
-                # 655,362-cell, 64-field case (FP16: 3.14 + 2.61 GB; TF32: 3.95 + 2.65 GB), scaled by the
+                # 655,362-cell, 64-field case (FP16: 4.01 + 2.76 GB; TF32: 3.95 + 2.65 GB), scaled by the
                 # cell count
-                "traffic": (5.750e9 if f16 else 6.600e9) * g.n / 655362 if F == 64 else None,
+                "traffic": (6.767e9 if f16 else 6.600e9) * g.n / 655362 if F == 64 else None,
                 "traffic_source": "ncu capture on 655,362 cells x 64 fields, scaled by cells",
                 "leaf_ms": leaf_ms, "proxy_ms": proxy_ms, "prep_upward_ms": up_ms}
     else:
@@ -700,9 +701,10 @@ def main():
                     "api": "sal_solve_host_async + sal_solve_host_wait (pinned host buffers, two staging slots)",
                     "sync_value": e2e_sync, "sync_api": "sal_solve_host"},
             "clocks": clocks,
-            # batched form per 64-field block: prep, split store (points), upward, finalize,
-            # split store (proxies), proxy, finalize, split store (potentials), leaf
-            "gpu_launches": 9 * args.steps * (((F + 63) // 64) if F > 32 else 1) if form == S.FORM_MIXED else 6 * args.steps,
+            # batched form: the library's count per block (prep, stores, upward, transfers, proxy,
+            # finalize, leaf); FP64 forms: prep, upward, finalize, proxy, finalize, leaf
+            "gpu_launches": (st_after["launches_batched"] * args.steps * (((F + 63) // 64) if F > 32 else 1)
+                             if form == S.FORM_MIXED else 6 * args.steps),
         }
         if cb:
             line["cpu_baseline"] = cb

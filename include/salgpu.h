@@ -142,6 +142,8 @@ typedef struct {
     double macs_up_batched, macs_down_batched;       /* the batched form's basis multiply-adds per field: the
                                                         leaf-level upward and DOWN work of its tree passes (or the
                                                         direct ones, as macs_up / macs_down, when those are off) */
+    int64_t launches_batched;                        /* kernel launches of one batched block under the current
+                                                        choices (sal_tune) */
 } sal_grid_stats;
 
 /* Runtime choices of the batched form's tcgen05 passes (no counterpart in the

@@ -390,6 +390,27 @@ static int64_t mixed_bytes_needed(const GridImpl &g, int FT) {
     return b;
 }
 
+// Kernel launches of one batched block of FT fields (solve_mixed_block's
+// sequence for the current plan).
+static int64_t batched_launches(const GridImpl &g, int FT) {
+    const Plan &pl = g.plan;
+    const bool tc = FT == 64 && !pl.tc_items.empty();
+    if (!tc) return 1 + (pl.mix_up_groups.empty() ? 0 : 2) + (pl.mix_proxy_groups.empty() ? 0 : 2) + 1;
+    const bool tree = pl.tc_opt.tree_passes != 0;
+    auto levels = [](const std::vector<int32_t> &beg) {
+        int64_t k = 0;
+        for (size_t l = 0; l + 1 < beg.size(); ++l) k += beg[l + 1] > beg[l];
+        return k;
+    };
+    int64_t k = 2;                                                         // prep, store (points)
+    if (!pl.tc_up_groups.empty()) k += tree ? 1 : 2;                       // upward (+ finalize)
+    if (tree) k += levels(pl.m2m_level_beg);
+    k += 1;                                                                // store (proxies)
+    if (!pl.tc_proxy_groups.empty()) k += 2 + (tree ? levels(pl.l2l_level_beg) : 0);   // proxy, finalize, l2l
+    k += pl.tc_opt.f16 ? 3 : 1;                                            // leaf store: maxima + FP16, or TF32
+    return k + 1;                                                          // leaf pass
+}
+
 extern "C" int sal_grid_stats_get(const sal_grid *G, sal_grid_stats *s) {
     if (!G || !s) return set_error(SAL_EINVAL, "null argument");
     const GridImpl &g = G->g;
@@ -412,6 +433,7 @@ extern "C" int sal_grid_stats_get(const sal_grid *G, sal_grid_stats *s) {
     s->macs_up_batched = pl.tc_items.empty() ? pl.macs_up : pl.tc_macs_up;
     s->macs_down_batched = pl.tc_items.empty() ? pl.macs_down : pl.tc_macs_down;
     s->mixed_bytes = g.FT ? g.mix_bytes : mixed_bytes_needed(g, g.max_fields <= 32 ? 32 : 64);
+    s->launches_batched = batched_launches(g, g.FT ? g.FT : (g.max_fields <= 32 ? 32 : 64));
     return SAL_OK;
 }
 

@@ -101,8 +101,7 @@ __global__ void __launch_bounds__(64 * N) m2m_kernel(const int32_t *__restrict__
 // Parent-to-child transfer of one tree level.  tasks: 4 per child (child
 // slot, parent slot, own: 1 adds to the child's own potentials, 0 replaces
 // them, the child's halves: bit 0 xi, bit 1 eta).  phi: per slot 3 N^2 rows
-// (proxy p, Cartesian component c at row 3p + c) of 64 fields.  One CTA per
-// (task, component c = blockIdx.y): the components' rows are disjoint.
+// (proxy p, Cartesian component c at row 3p + c) of 64 fields.
 template <int N>
 __global__ void __launch_bounds__(64 * N) l2l_kernel(const int32_t *__restrict__ tasks, const double *__restrict__ H,
                                                      float *__restrict__ phi) {
@@ -117,8 +116,8 @@ __global__ void __launch_bounds__(64 * N) l2l_kernel(const int32_t *__restrict__
     const double *A = Hs + (code & 1) * P, *B = Hs + ((code >> 1) & 1) * P;
     const float *src = phi + (size_t)parent * 3 * P * kF;
     float *dst = phi + (size_t)child * 3 * P * kF;
-    {
-        const int c = blockIdx.y;
+    for (int c = 0; c < 3; ++c) {
+        __syncthreads();
         for (int e = tid; e < P * kF; e += 64 * N) Pp[e] = src[((size_t)3 * (e / kF) + c) * kF + (e % kF)];
         __syncthreads();
         // T(r, l) = sum_k B[k][l] Phi_p(r, k)
@@ -163,7 +162,7 @@ template <int N>
 static void launch_l2l_n(const int32_t *tasks, int ntasks, const double *H, float *phi, cudaStream_t st) {
     static std::atomic<unsigned long long> done{0};
     smem_attr_once((const void *)l2l_kernel<N>, (int)transfer_smem<N>(), done);
-    l2l_kernel<N><<<dim3(ntasks, 3), 64 * N, transfer_smem<N>(), st>>>(tasks, H, phi);
+    l2l_kernel<N><<<ntasks, 64 * N, transfer_smem<N>(), st>>>(tasks, H, phi);
 }
 
 // N = d + 1 from 2 to kMaxTreeDegree + 1 (the plan turns the tree passes off

@@ -69,7 +69,7 @@ class GridStats(C.Structure):
         ("pairs_pp", C.c_double), ("pairs_pc", C.c_double), ("pairs_cp", C.c_double), ("pairs_cc", C.c_double),
         ("macs_up", C.c_double), ("macs_down", C.c_double),
         ("device_bytes", C.c_int64), ("setup_seconds", C.c_double), ("mixed_bytes", C.c_int64),
-        ("macs_up_batched", C.c_double), ("macs_down_batched", C.c_double),
+        ("macs_up_batched", C.c_double), ("macs_down_batched", C.c_double), ("launches_batched", C.c_int64),
     ]
 
 
