@@ -122,7 +122,7 @@ class Server:
 
     def __init__(self, hbm_budget_bytes: int, max_batch: int = 64, device: int = 0, clock=time.perf_counter,
                  grid_factory=Grid, priorities: bool = True, patience: float = 2.0, graphs: bool = False,
-                 device_setup: bool = True):
+                 device_setup: bool = True, tune: dict | None = None):
         try:
             import torch
         except ImportError:           # the CPU test double needs no torch
@@ -142,6 +142,10 @@ class Server:
         self.patience = float(patience)
         self.graphs = graphs                 # one CUDA graph per (grid, batch width)
         self.device_setup = device_setup     # tree and list built on the device when one is present
+        # batched-form choices set on every admitted grid (sal_grid_tune_set): FP16 leaf operands and
+        # 64-unit chains, the autotuner's pick on the 2.3M-cell grid; one group per CTA keeps the
+        # CTAs short, so higher-priority grids' kernels get SMs quickly
+        self.tune = dict(f16=1, chain_ksteps=64) if tune is None else dict(tune)
         self.batches: list[tuple] = []     # (grid, fields, launch time, done time) of finished batches
 
     # ------------------------------------------------------------------ grids
@@ -181,6 +185,8 @@ class Server:
         s = r.spec
         g = self.grid_factory(r.tree, s.xs, s.ys, s.zs, s.areas, s.degree, MODE_DTT, r.inter, device=self.device,
                               max_fields=self.max_batch)
+        if self.tune and hasattr(g, "tune"):
+            g.tune(**self.tune)
         need = self._bytes_needed(r, g)
         if need > self.budget:
             del g
