@@ -55,6 +55,8 @@ def _args():
     ap.add_argument("--serve-rate", type=float, default=200.0)
     ap.add_argument("--serve-host", action="store_true", help="serving requests carry host arrays")
     ap.add_argument("--no-serve", action="store_true")
+    ap.add_argument("--serve-tune", default=None,
+                    help="batched-form settings of the served grids as name=value,... (default: the server's)")
     ap.add_argument("--no-autotune", action="store_true", help="time the batched form's default settings")
     ap.add_argument("--tune", default=None,
                     help="batched form's settings as name=value,... (sal_tune fields); replaces the autotuner")
@@ -409,7 +411,8 @@ def serving_run(args, S, torch, dev):
     from salgpu import serve, synth
     sizes = {"serve_40962": 40962, "serve_163842": 163842, "serve_655362": 655362, "serve_2313486": 2313486}
     weights = {"serve_40962": 0.4, "serve_163842": 0.3, "serve_655362": 0.2, "serve_2313486": 0.1}
-    srv = serve.Server(60 << 30, max_batch=64, device=dev.index or 0)
+    tune = None if not args.serve_tune else {k: int(v) for k, v in (kv.split("=") for kv in args.serve_tune.split(","))}
+    srv = serve.Server(60 << 30, max_batch=64, device=dev.index or 0, tune=tune)
     pools, grids = {}, {}
     for name in sizes:
         g = synth.config_grid(name, device=dev)
