@@ -336,3 +336,21 @@ def test_f16_joint_solve_equals_separate_solves_and_memory_estimate():
     torch.cuda.synchronize()
     for grid, (ox, oy) in zip(grids, outs):
         assert torch.equal(ox, grid.sep[0]) and torch.equal(oy, grid.sep[1])
+
+
+def test_f16_batch_invariance_and_zero_field():
+    """FP16 leaf operands: every field's scale is its own, so a field's result
+    is the same bit for bit alone and inside a batch of fields of any
+    amplitude, and an all-zero field gives exact zeros (scale 1, no NaN)."""
+    torch = _torch()
+    S, g, hs, grid = _grid("small_3000", 20, 5, seed=17, max_fields=64)
+    hs = hs * np.array([1.0, 1e4, 1e-5, 0.0, 3.0])[:, None]
+    ssh = torch.tensor(hs, device="cuda")
+    grid.tune(f16=1)
+    bx, by = grid.solve(ssh, form=S.FORM_MIXED)
+    torch.cuda.synchronize()
+    assert torch.count_nonzero(bx[3]) == 0 and torch.count_nonzero(by[3]) == 0
+    for f in (0, 2, 4):
+        ox, oy = grid.solve(ssh[f:f + 1], form=S.FORM_MIXED)
+        torch.cuda.synchronize()
+        assert torch.equal(ox[0], bx[f]) and torch.equal(oy[0], by[f])
