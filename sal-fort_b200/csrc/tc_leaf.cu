@@ -992,30 +992,49 @@ __global__ void field_max_kernel(const float4 *__restrict__ x, int64_t nrows, un
 // one 128-row FP16 tile (field f's hi part at row wrow(f, 0), lo at
 // wrow(f, 1); row m at byte (m / 8) 128 + (m % 8) 16, 8 halves), source
 // weights scaled by their field's power of two, potentials by theirs.  One
-// thread per (unit, field).
+// thread per (unit, 4 fields): float4 row loads, 64-byte row-group stores.
 __global__ void split_store16_kernel(const int32_t *__restrict__ bsrc, int64_t nu, const float *__restrict__ wF,
                                      const float *__restrict__ phiF, const unsigned *__restrict__ fmax,
                                      unsigned char *__restrict__ out) {
     const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= nu * kF) return;
-    const int64_t u = t / kF;
-    const int f = (int)(t % kF);
-    const float sw = f16_scale(__uint_as_float(fmax[f])), sp = f16_scale(__uint_as_float(fmax[kF + f]));
-    float v[8];
+    if (t >= nu * (kF / 4)) return;
+    const int64_t u = t / (kF / 4);
+    const int f0 = 4 * (int)(t % (kF / 4));
+    float sw[4], sp[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        sw[i] = f16_scale(__uint_as_float(fmax[f0 + i]));
+        sp[i] = f16_scale(__uint_as_float(fmax[kF + f0 + i]));
+    }
+    float v[4][8];   // [field][row]
 #pragma unroll
     for (int r = 0; r < 8; ++r) {
         const int32_t s = bsrc[u * 8 + r];
-        v[r] = s >= 0 ? wF[(size_t)s * kF + f] * sw : (s <= -2 ? phiF[(size_t)(-2 - s) * kF + f] * sp : 0.f);
+        float4 x = make_float4(0.f, 0.f, 0.f, 0.f);
+        const float *sc = sw;
+        if (s >= 0) {
+            x = *reinterpret_cast<const float4 *>(wF + (size_t)s * kF + f0);
+        } else if (s <= -2) {
+            x = *reinterpret_cast<const float4 *>(phiF + (size_t)(-2 - s) * kF + f0);
+            sc = sp;
+        }
+        v[0][r] = x.x * sc[0];
+        v[1][r] = x.y * sc[1];
+        v[2][r] = x.z * sc[2];
+        v[3][r] = x.w * sc[3];
     }
-    uint4 hi, lo;
-    split_f16x2(v[0], v[1], hi.x, lo.x);
-    split_f16x2(v[2], v[3], hi.y, lo.y);
-    split_f16x2(v[4], v[5], hi.z, lo.z);
-    split_f16x2(v[6], v[7], hi.w, lo.w);
     unsigned char *base = out + u * kW16UnitBytes;
-    const int mh = wrow(f, 0), ml = wrow(f, 1);
-    *reinterpret_cast<uint4 *>(base + (mh >> 3) * 128 + (mh & 7) * 16) = hi;
-    *reinterpret_cast<uint4 *>(base + (ml >> 3) * 128 + (ml & 7) * 16) = lo;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        uint4 hi, lo;
+        split_f16x2(v[i][0], v[i][1], hi.x, lo.x);
+        split_f16x2(v[i][2], v[i][3], hi.y, lo.y);
+        split_f16x2(v[i][4], v[i][5], hi.z, lo.z);
+        split_f16x2(v[i][6], v[i][7], hi.w, lo.w);
+        const int mh = wrow(f0 + i, 0), ml = wrow(f0 + i, 1);
+        *reinterpret_cast<uint4 *>(base + (mh >> 3) * 128 + (mh & 7) * 16) = hi;
+        *reinterpret_cast<uint4 *>(base + (ml >> 3) * 128 + (ml & 7) * 16) = lo;
+    }
 }
 
 // FP16 leaf pass: per target the power of two that takes its largest kernel
@@ -1205,7 +1224,7 @@ void launch_field_max(const float *wF, int64_t nw, const float *phiF, int64_t np
 void launch_split_store16(const int32_t *bsrc, int64_t nunits, const float *wF, const float *phiF,
                           const unsigned *fmax, void *bstore16, cudaStream_t st) {
     if (nunits <= 0) return;
-    const int64_t threads = nunits * kF;
+    const int64_t threads = nunits * (kF / 4);
     split_store16_kernel<<<(unsigned)((threads + 255) / 256), 256, 0, st>>>(bsrc, nunits, wF, phiF, fmax,
                                                                             static_cast<unsigned char *>(bstore16));
 }
