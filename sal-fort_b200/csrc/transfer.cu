@@ -16,8 +16,10 @@
 //     -- the parent's potential interpolant evaluated at the child's nodes,
 //     so the child's interpolant reproduces it.
 // Both are exact in exact arithmetic.  Each is two 1-D transfers (2 N^3
-// multiply-adds per field instead of N^4), summed in FP64 and stored in FP32
-// like the rows they read.  One CTA of 64 N threads per task: thread
+// multiply-adds per field instead of N^4), in FP32 like the rows they read
+// and write (a transfer rounds at the 1e-7 level; FP64 sums made the solve
+// 0.35 ms slower at 2.3M cells x 64 fields and were no more accurate against
+// the direct sum).  One CTA of 64 N threads per task: thread
 // (f = t % 64, r = t / 64) keeps row r of the tile for field f in registers,
 // so every shared-memory value it loads feeds N multiply-adds, and the loops
 // are unrolled over the compile-time N.
@@ -34,8 +36,8 @@ constexpr int kF = 64;
 
 template <int N>
 constexpr size_t transfer_smem() {
-    // both matrices, a float tile and a double tile
-    return (2 * N * N + (size_t)N * N * kF) * sizeof(double) + (size_t)N * N * kF * sizeof(float);
+    // both matrices and two float tiles
+    return (2 * N * N + 2 * (size_t)N * N * kF) * sizeof(float);
 }
 }  // namespace
 
@@ -47,55 +49,54 @@ template <int N>
 __global__ void __launch_bounds__(64 * N) m2m_kernel(const int32_t *__restrict__ tasks, const double *__restrict__ H,
                                                      float *__restrict__ w) {
     constexpr int P = N * N;
-    extern __shared__ __align__(16) double sm[];
-    double *Hs = sm, *T = Hs + 2 * P;
-    float *Wc = reinterpret_cast<float *>(T + (size_t)P * kF);
+    extern __shared__ __align__(16) float smf[];
+    float *Hs = smf, *T = Hs + 2 * P, *Wc = T + (size_t)P * kF;
     const int32_t *tk = tasks + 6 * (size_t)blockIdx.x;
     const int tid = threadIdx.x, f = tid & (kF - 1), r = tid >> 6;
-    for (int e = tid; e < 2 * P; e += 64 * N) Hs[e] = H[e];
-    double acc[N];   // W_p(j, r), j = 0 .. N-1
+    for (int e = tid; e < 2 * P; e += 64 * N) Hs[e] = (float)H[e];
+    float acc[N];   // W_p(j, r), j = 0 .. N-1
 #pragma unroll
-    for (int j = 0; j < N; ++j) acc[j] = 0.0;
+    for (int j = 0; j < N; ++j) acc[j] = 0.f;
     const int code = tk[5];
     for (int c = 0; c < 4; ++c) {
         const int child = tk[1 + c];
         if (child < 0) continue;
-        const double *A = Hs + ((code >> (2 * c)) & 1) * P, *B = Hs + ((code >> (2 * c + 1)) & 1) * P;
+        const float *A = Hs + ((code >> (2 * c)) & 1) * P, *B = Hs + ((code >> (2 * c + 1)) & 1) * P;
         __syncthreads();   // the previous child's tiles are consumed
         const float *src = w + (size_t)child * P * kF;
         for (int e = tid; e < P * kF; e += 64 * N) Wc[e] = src[e];
         __syncthreads();
         // T(r, k) = sum_l B[k][l] W_c(r, l)
         {
-            double wv[N];
+            float wv[N];
 #pragma unroll
-            for (int l = 0; l < N; ++l) wv[l] = (double)Wc[(r + l * N) * kF + f];
+            for (int l = 0; l < N; ++l) wv[l] = Wc[(r + l * N) * kF + f];
 #pragma unroll
             for (int k = 0; k < N; ++k) {
-                double s = 0.0;
+                float s = 0.f;
 #pragma unroll
-                for (int l = 0; l < N; ++l) s = fma(B[k * N + l], wv[l], s);
+                for (int l = 0; l < N; ++l) s = fmaf(B[k * N + l], wv[l], s);
                 T[(r + k * N) * kF + f] = s;
             }
         }
         __syncthreads();
         // W_p(j, r) += sum_i A[j][i] T(i, r)
         {
-            double tv[N];
+            float tv[N];
 #pragma unroll
             for (int i = 0; i < N; ++i) tv[i] = T[(i + r * N) * kF + f];
 #pragma unroll
             for (int j = 0; j < N; ++j) {
-                double s = 0.0;
+                float s = 0.f;
 #pragma unroll
-                for (int i = 0; i < N; ++i) s = fma(A[j * N + i], tv[i], s);
+                for (int i = 0; i < N; ++i) s = fmaf(A[j * N + i], tv[i], s);
                 acc[j] += s;
             }
         }
     }
     float *dst = w + (size_t)tk[0] * P * kF;
 #pragma unroll
-    for (int j = 0; j < N; ++j) dst[(j + r * N) * kF + f] = (float)acc[j];
+    for (int j = 0; j < N; ++j) dst[(j + r * N) * kF + f] = acc[j];
 }
 
 // Parent-to-child transfer of one tree level.  tasks: 4 per child (child
@@ -106,14 +107,13 @@ template <int N>
 __global__ void __launch_bounds__(64 * N) l2l_kernel(const int32_t *__restrict__ tasks, const double *__restrict__ H,
                                                      float *__restrict__ phi) {
     constexpr int P = N * N;
-    extern __shared__ __align__(16) double sm[];
-    double *Hs = sm, *T = Hs + 2 * P;
-    float *Pp = reinterpret_cast<float *>(T + (size_t)P * kF);
+    extern __shared__ __align__(16) float smf[];
+    float *Hs = smf, *T = Hs + 2 * P, *Pp = T + (size_t)P * kF;
     const int32_t *tk = tasks + 4 * (size_t)blockIdx.x;
     const int child = tk[0], parent = tk[1], own = tk[2], code = tk[3];
     const int tid = threadIdx.x, f = tid & (kF - 1), r = tid >> 6;
-    for (int e = tid; e < 2 * P; e += 64 * N) Hs[e] = H[e];
-    const double *A = Hs + (code & 1) * P, *B = Hs + ((code >> 1) & 1) * P;
+    for (int e = tid; e < 2 * P; e += 64 * N) Hs[e] = (float)H[e];
+    const float *A = Hs + (code & 1) * P, *B = Hs + ((code >> 1) & 1) * P;
     const float *src = phi + (size_t)parent * 3 * P * kF;
     float *dst = phi + (size_t)child * 3 * P * kF;
     for (int c = 0; c < 3; ++c) {
@@ -122,30 +122,30 @@ __global__ void __launch_bounds__(64 * N) l2l_kernel(const int32_t *__restrict__
         __syncthreads();
         // T(r, l) = sum_k B[k][l] Phi_p(r, k)
         {
-            double pv[N];
+            float pv[N];
 #pragma unroll
-            for (int k = 0; k < N; ++k) pv[k] = (double)Pp[(r + k * N) * kF + f];
+            for (int k = 0; k < N; ++k) pv[k] = Pp[(r + k * N) * kF + f];
 #pragma unroll
             for (int l = 0; l < N; ++l) {
-                double s = 0.0;
+                float s = 0.f;
 #pragma unroll
-                for (int k = 0; k < N; ++k) s = fma(B[k * N + l], pv[k], s);
+                for (int k = 0; k < N; ++k) s = fmaf(B[k * N + l], pv[k], s);
                 T[(r + l * N) * kF + f] = s;
             }
         }
         __syncthreads();
         // Phi_c(i, r) (+)= sum_j A[j][i] T(j, r)
         {
-            double tv[N];
+            float tv[N];
 #pragma unroll
             for (int j = 0; j < N; ++j) tv[j] = T[(j + r * N) * kF + f];
 #pragma unroll
             for (int i = 0; i < N; ++i) {
-                double s = 0.0;
+                float s = 0.f;
 #pragma unroll
-                for (int j = 0; j < N; ++j) s = fma(A[j * N + i], tv[j], s);
+                for (int j = 0; j < N; ++j) s = fmaf(A[j * N + i], tv[j], s);
                 float *out = dst + ((size_t)3 * (i + r * N) + c) * kF + f;
-                *out = own ? (float)((double)*out + s) : (float)s;
+                *out = own ? *out + s : s;
             }
         }
     }
