@@ -144,6 +144,8 @@ typedef struct {
                                                         direct ones, as macs_up / macs_down, when those are off) */
     int64_t launches_batched;                        /* kernel launches of one batched block under the current
                                                         choices (sal_tune) */
+    int64_t tile_store_bytes;                        /* device bytes of the FP16 leaf pass's kernel-tile store under
+                                                        the current plan (allocated only with sal_tune.tile_store) */
 } sal_grid_stats;
 
 /* Runtime choices of the batched form's tcgen05 passes (no counterpart in the
@@ -161,6 +163,11 @@ typedef struct {
     int32_t field_block;        /* fields per block: 64 (tcgen05 passes) or 32 (mma.sync passes) */
     int32_t f16;                /* 64-field leaf pass: 1 FP16 hi/lo operands (16 sources per MMA), scaled per field and
                                    per target by powers of two; 0 TF32 hi/lo (8 sources per MMA) */
+    int32_t tile_store;         /* FP16 leaf pass: 1 keeps its kernel tiles (the near-field and proxy kernel values and
+                                   DOWN interpolation rows, FP16 hi/lo, which depend on the grid alone) in device
+                                   memory, sal_grid_stats.tile_store_bytes of it: the first solve records them, later
+                                   solves read them instead of computing them, with the same results bit for bit.
+                                   Allocated with the batched buffers; ignored with f16 = 0 or 32-field blocks */
 } sal_tune;
 
 /* Flattens the tree and lists into device-resident arrays (once per grid). */

@@ -77,6 +77,9 @@ struct GridImpl {
     void *bstore16 = nullptr;         // FP16 leaf pass: its FP16 hi/lo weight store (one spare unit at the end)
     float *tscale = nullptr, *tinv = nullptr;   // FP16 leaf pass: per target, its kernel values' scale
     unsigned *fmax = nullptr;         // FP16 leaf pass: the block's field maxima (source weights, potentials)
+    unsigned char *ktile = nullptr;   // FP16 leaf pass with sal_tune.tile_store: its kernel tiles
+    int64_t *ktile_off = nullptr;     // per leaf group, the byte offset of its tiles
+    bool tile_recorded = false;       // a solve has been launched that records the tiles
     float4 *sloc = nullptr;
     float *sxyz = nullptr;
     int32_t *iperm = nullptr;         // caller index -> pool position
@@ -217,6 +220,7 @@ static int release_mixed(GridImpl &g) {
     g.mix_allocs.clear();
     g.FT = 0;
     g.mix_bytes = 0;
+    g.tile_recorded = false;
     // captured graphs name the freed buffers
     std::lock_guard<std::mutex> lk(g.graph_mu);
     for (auto &e : g.graphs) cudaGraphExecDestroy(e.exec);
@@ -386,6 +390,7 @@ static int64_t mixed_bytes_needed(const GridImpl &g, int FT) {
              (int64_t)sizeof(float4) * (n + (int64_t)g.nsrc * P) + (int64_t)sizeof(double2) * n +
              4 * pl.tc_src_ksteps * 24;
         if (pl.tc_opt.f16) b += ((int64_t)pl.bsrc.size() / 8 + 1) * 2048 + 128 * 4 + 2 * 4 * n;
+        if (pl.tc_opt.f16 && pl.tc_opt.tile_store) b += pl.tc_tile_off.back() + vb(pl.tc_tile_off);
     }
     return b;
 }
@@ -434,6 +439,7 @@ extern "C" int sal_grid_stats_get(const sal_grid *G, sal_grid_stats *s) {
     s->macs_down_batched = pl.tc_items.empty() ? pl.macs_down : pl.tc_macs_down;
     s->mixed_bytes = g.FT ? g.mix_bytes : mixed_bytes_needed(g, g.max_fields <= 32 ? 32 : 64);
     s->launches_batched = batched_launches(g, g.FT ? g.FT : (g.max_fields <= 32 ? 32 : 64));
+    s->tile_store_bytes = pl.tc_tile_off.empty() ? 0 : pl.tc_tile_off.back();
     return SAL_OK;
 }
 
@@ -622,6 +628,12 @@ static int ensure_mixed(GridImpl &g, int FT) {
                 CK(cudaStreamSynchronize(g.stream));
                 CK(cudaGetLastError());
             }
+            // the kernel-tile store, written by the next leaf pass
+            if (!rc && pl.tc_opt.tile_store) {
+                rc = upload_mix(g, &g.ktile_off, pl.tc_tile_off);
+                if (!rc) rc = malloc_mix(g, &g.ktile, (size_t)pl.tc_tile_off.back());
+                g.tile_recorded = false;
+            }
         }
         if (!rc) CK(cudaDeviceGetAttribute(&g.nsm, cudaDevAttrMultiProcessorCount, g.dev));
     }
@@ -661,6 +673,8 @@ static mix::TcArgs leaf_args(GridImpl &g, double *ox, double *oy, int64_t ld_out
         t.tscale = g.tscale;
         t.tinv = g.tinv;
         t.fmax = g.fmax;
+        t.ktile = g.ktile;
+        t.ktile_off = g.ktile_off;
     }
     return t;
 }
@@ -779,7 +793,11 @@ static void solve_mixed_block(GridImpl &g, const double *ssh, int64_t ld_ssh, in
     if (g.bstore) {
         // 64-field blocks: the leaf pass's weight rows, then the tcgen05 leaf pass
         leaf_store();
-        mix::launch_tc_leaf(leaf_args(g, ox, oy, ld_out, f0, nf), g.nsm, cg, g.err, st);
+        // with a kernel-tile store: the first leaf pass records the tiles, the
+        // later ones (stream-ordered after it) replay them
+        const int tiles = g.ktile ? (g.tile_recorded ? 2 : 1) : 0;
+        mix::launch_tc_leaf(leaf_args(g, ox, oy, ld_out, f0, nf), g.nsm, cg, g.err, st, tiles);
+        if (tiles == 1) g.tile_recorded = true;
     } else {
         a.groups = g.mix_leaf_groups;
         mix::launch_mix(0, FT, a, (int)pl.mix_leaf_groups.size(), st);
@@ -806,6 +824,9 @@ constexpr size_t kMaxGraphs = 128;
 // kernels keep.  Every allocation and kernel attribute the solve needs exists
 // already: the same shape has just run.  Called with graph_mu held.
 static int capture_mixed(GridImpl &g, const GridImpl::GraphShape &k, cudaStream_t caller) {
+    // a graph replays its launches as captured: the tile store's recording
+    // pass must not be one of them
+    if (g.ktile && !g.tile_recorded) return SAL_OK;
     int prio = 0;
     CK(cudaStreamGetPriority(caller, &prio));
     cudaStream_t cs = nullptr;
@@ -943,6 +964,7 @@ static sal_tune tune_of(const GridImpl &g) {
     t.cta_groups = o.cta_groups;
     t.field_block = g.FT ? g.FT : (g.max_fields <= 32 ? 32 : 64);
     t.f16 = o.f16;
+    t.tile_store = o.tile_store;
     return t;
 }
 
@@ -955,6 +977,7 @@ static int apply_tune(GridImpl &g, const sal_tune &t) {
     o.proxy_unit_kpairs = t.proxy_unit_kpairs;
     o.cta_groups = t.cta_groups;
     o.f16 = t.f16 ? 1 : 0;
+    o.tile_store = t.tile_store ? 1 : 0;
     const TcOptions &c = g.plan.tc_opt;
     const bool same_plan = o.chain_ksteps == c.chain_ksteps && o.tree_passes == c.tree_passes &&
                            o.up_chunk == c.up_chunk && o.proxy_unit_kpairs == c.proxy_unit_kpairs &&
@@ -962,7 +985,14 @@ static int apply_tune(GridImpl &g, const sal_tune &t) {
     const int cur_block = g.FT ? g.FT : (g.max_fields <= 32 ? 32 : 64);
     if (same_plan && t.field_block == cur_block) {
         if (o.cta_groups < 1) return set_error(SAL_EINVAL, "tcgen05 options must be positive");
+        // the tile store is allocated with the batched buffers: switching it
+        // frees them (the next solve allocates them again)
+        if (o.tile_store != c.tile_store) {
+            int rc = release_mixed(g);
+            if (rc) return rc;
+        }
         g.plan.tc_opt.cta_groups = o.cta_groups;
+        g.plan.tc_opt.tile_store = o.tile_store;
         return SAL_OK;
     }
     int rc = release_mixed(g);
@@ -973,6 +1003,7 @@ static int apply_tune(GridImpl &g, const sal_tune &t) {
         if (!plan_build_tc(g.tree, &g.plan, o, &err)) return set_error(SAL_EINVAL, err);
     } else {
         g.plan.tc_opt.cta_groups = o.cta_groups;
+        g.plan.tc_opt.tile_store = o.tile_store;
     }
     if (t.field_block == 32 && !g.plan.mix_built) plan_build_mix(g.tree, &g.plan);
     return SAL_OK;
@@ -1151,6 +1182,7 @@ static int finish(GridImpl &g, cudaStream_t st) {
     CK(cudaStreamSynchronize(st));
     const int flag = *g.h_flag;
     if (flag) {
+        g.tile_recorded = false;   // a recording pass may have given up: record again
         cudaMemsetAsync(g.err, 0, sizeof(int), st);
         cudaStreamSynchronize(st);
         return set_error(SAL_ETIMEOUT, "a staging wait timed out on the device");

@@ -73,6 +73,10 @@ struct TcArgs {
     const void *bstore16;
     const float *tscale, *tinv;
     const unsigned *fmax;
+    // FP16 leaf pass with a kernel-tile store: the store and per group the
+    // byte offset of its tiles (ngroups + 1 entries)
+    unsigned char *ktile;
+    const int64_t *ktile_off;
 };
 // cta_groups: groups one CTA walks at most (the grid has every SM busy
 // otherwise)
@@ -83,7 +87,9 @@ struct TcJoint {
     int32_t beg[kMaxJoint + 1];   // first joint group of each grid; beg[ngrids] = all groups
     int32_t ngrids;
 };
-void launch_tc_leaf(const TcArgs &a, int nsm, int cta_groups, int *err, cudaStream_t st);
+// tiles (FP16 leaf pass with a.ktile set): 0 computes the kernel tiles,
+// 1 computes them and records them in a.ktile, 2 replays them from a.ktile
+void launch_tc_leaf(const TcArgs &a, int nsm, int cta_groups, int *err, cudaStream_t st, int tiles = 0);
 void launch_tc_leaf_joint(const TcArgs *grids, int ngrids, int nsm, int cta_groups, int *err, cudaStream_t st);
 void launch_tc_proxy(const TcArgs &a, int nsm, int cta_groups, int *err, cudaStream_t st);
 void launch_tc_upward(const TcArgs &a, int nsm, int cta_groups, int *err, cudaStream_t st);

@@ -685,6 +685,19 @@ bool plan_build_tc(const Tree &t, Plan *pl, const TcOptions &opt, std::string *e
         }
     }
     if (!tree) pl->tc_macs_down = pl->macs_down;
+    // Kernel-tile store of the FP16 leaf pass: a group's tiles follow its
+    // items (one stage each: kTcChunk sources at most); a stage of c sources
+    // holds ceil(ceil(c / 8) / 2) MMA steps of 16 sources, each four chunks
+    // (hi, lo x east, north) of the group's rows rounded up to 16, 32 bytes
+    // per row.
+    pl->tc_tile_off.assign(pl->tc_leaf_groups.size() + 1, 0);
+    for (size_t gi = 0; gi < pl->tc_leaf_groups.size(); ++gi) {
+        const MixGroup &m = pl->tc_leaf_groups[gi];
+        const int64_t cb = (int64_t)((m.nt + 15) & ~15) * 32;
+        int64_t b = 0;
+        for (int32_t i = m.ib; i < m.ie; ++i) b += (int64_t)(((pl->tc_items[i].cnt + 7) / 8 + 1) / 2) * 4 * cb;
+        pl->tc_tile_off[gi + 1] = pl->tc_tile_off[gi] + b;
+    }
 
     // ---- proxy pass: each target slot's items cut into units of at most
     // proxy_unit_kpairs * 1024 pairs; rows of at most kTcProxyRows proxies

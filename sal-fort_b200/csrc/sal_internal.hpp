@@ -116,6 +116,9 @@ struct TcOptions {
     int32_t cta_groups = 1;             // tcgen05 launches: groups a CTA walks at most
     int32_t f16 = 0;                    // leaf pass: 1: FP16 hi/lo operands (kind::f16, 16 sources per MMA)
                                         //    with power-of-two scales; 0: TF32 hi/lo (8 sources per MMA)
+    int32_t tile_store = 0;             // FP16 leaf pass: 1: its kernel tiles are kept in device memory
+                                        //    (recorded by the first solve, replayed after); the plan is the
+                                        //    same either way
 };
 
 struct Plan {
@@ -150,6 +153,9 @@ struct Plan {
     // if >= 0, phiF row -2-v if <= -2, zero row if -1; every leaf, source
     // slot and target slot starts on a multiple of 8 rows).
     std::vector<MixGroup> tc_leaf_groups;
+    // FP16 kernel-tile store: per leaf group the byte offset of its tiles
+    // (ngroups + 1 entries; the last is the store's size)
+    std::vector<int64_t> tc_tile_off;
     std::vector<TcItem> tc_items;
     // tcgen05 proxy pass: per proxy unit, row chunks of at most kTcProxyRows
     // target proxies (row0 = first proxy, out = unit), and their items

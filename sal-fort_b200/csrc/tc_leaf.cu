@@ -102,18 +102,49 @@ constexpr int kStageKF16 = 64;
 constexpr int kW16UnitBytes = 2048;
 // FP16 operands are scaled by powers of two to at most 2^12 (FP16 max 65504)
 constexpr int kF16TopExp = 12;
+static_assert(kStageKF16 == kTcChunk, "an FP16 stage is one item: the tile store's layout");
 
+// Replay of the kernel-tile store: the stages' kernel tiles and weight tiles
+// go into two byte rings (a stage takes its own size, so the small groups'
+// stages do not hold whole 64 KB slots), with up to kRStages stages in
+// flight.  A stage's tiles are packed: per MMA step and hi / lo, the group's
+// east rows then its north rows (rows rounded up to 16); an MMA reads 256
+// rows from a tile's start, the rows past the group's are columns no fold
+// reads.
+constexpr int kRStages = 8;
+constexpr int kTRingBytes = 180 * 1024;
+constexpr int kWRingBytes = 44 * 1024;
+
+// Shared memory of one CTA.  Computing launches: a kKStages-deep ring of
+// 64 KB kernel-tile stages, a kWStages-deep weight ring and the producers'
+// buffers (source coordinates / upward factors per weight stage, DOWN bases,
+// the DOWN row map).  Replay: the two byte rings and the offsets of the
+// stages in flight.
+template <int TS>
 struct TcSmem {
-    float Kt[kKStages][kStageKs][2][kTileFloats];   // per stage: k-step x {hi, lo} x 256 rows x 8
-    float Wt[kWStages][kStageKs * kWStepFloats];    // per stage: k-steps x 128 weight rows x 8
-    float aux[kWStages][kAuxFloats];                // per stage: BLI factors F[n][8] G[n][8] per k-step (upward)
-    float fx[kTcRows][kMaxDegree + 1];              // per target row: BLI bases in the current DOWN slot
-    float fe[kTcRows][kMaxDegree + 1];
-    int kmap[kKmap];
-    uint64_t kfull[kKStages], kempty[kKStages], wfull[kWStages], wempty[kWStages], accfull, accfree, fin;
+    static constexpr bool kReplay = TS == 2;
+    static constexpr int KS = kReplay ? kRStages : kKStages;   // kernel-tile stage slots
+    static constexpr int WS = kReplay ? 1 : kWStages;          // weight stage slots
+    static constexpr size_t kKtBytes = kReplay ? (size_t)kTRingBytes : (size_t)kKStages * kStageKs * 2 * kTileFloats * 4;
+    static constexpr size_t kWtBytes = kReplay ? (size_t)kWRingBytes : (size_t)kWStages * kStageKs * kWStepFloats * 4;
+    unsigned char ring[kKtBytes + kWtBytes];
+    float aux[kReplay ? 1 : kWStages][kReplay ? 4 : kAuxFloats];   // per stage: BLI factors F[n][8] G[n][8] per k-step
+    float fx[kReplay ? 1 : kTcRows][kMaxDegree + 1];              // per target row: BLI bases in the current DOWN slot
+    float fe[kReplay ? 1 : kTcRows][kMaxDegree + 1];
+    int kmap[kReplay ? 1 : kKmap];
+    uint32_t toff[KS], tlen[KS], woff[KS], wlen[KS];             // replay: each stage slot's ranges in the rings
+    uint64_t kfull[KS], kempty[KS], wfull[WS], wempty[WS], accfull, accfree, fin;
     uint32_t tmem_base;
     int abort;
+    // computing launches: kernel tile (stage slot, k-step, hi / lo), weight stage jb
+    __device__ __forceinline__ float *Kt(uint32_t slot, int s, int h) {
+        return reinterpret_cast<float *>(ring + (((size_t)slot * kStageKs + s) * 2 + h) * kTileFloats * 4);
+    }
+    __device__ __forceinline__ float *Wt(uint32_t jb) {
+        return reinterpret_cast<float *>(ring + kKtBytes + (size_t)jb * kStageKs * kWStepFloats * 4);
+    }
 };
+template <int TS> constexpr size_t tc_smem_need() { return sizeof(TcSmem<TS>) + 1024; }
 
 
 // Packed FP32x2 arithmetic (two kernel-tile columns per instruction).
@@ -289,14 +320,14 @@ __host__ __device__ constexpr int wrow(int f, int part) { return 32 * (f >> 4) +
 // so hi + lo of a field meet in one lane.
 template <int MODE>
 __device__ __forceinline__ void emit_chunk(const float (&x)[16], int c0, int f, int odd, int nt, int idk, double *out,
-                                           bool wr, float *part) {
+                                           bool wr, float *part, int half) {
 #pragma unroll
     for (int m = 0; m < 8; ++m) {
         const float lo_even = __shfl_down_sync(0xffffffffu, x[2 * m], 16);
         const float hi_odd = __shfl_up_sync(0xffffffffu, x[2 * m + 1], 16);
         const int j = c0 + 2 * m + odd;   // column
         if (MODE == 0) {
-            const int t = j & 127;
+            const int t = j >= half ? j - half : j;
             const int ti = __shfl_sync(0xffffffffu, idk, t & 31);
             const double v = odd ? (double)hi_odd + (double)x[2 * m + 1] : (double)x[2 * m] + (double)lo_even;
             if (wr && t < nt) out[ti] = v;
@@ -323,33 +354,51 @@ __device__ __forceinline__ void emit_chunk(const float (&x)[16], int c0, int f, 
 // lo rows apart: mid-group, running sum (+)= chain with round-to-nearest FP32
 // adds (the group's first chain stores); at the group's end, running sum +
 // chain goes to the caller's outputs, hi + lo added in FP64.
-// MODE 0 (leaf): columns 128c + t are component c (east, north) of target t,
-// ends go to the caller's outputs.  MODE 1 (proxy): columns 85c + r are
+// MODE 0 (leaf): columns half c + t are component c (east, north) of target
+// t (half = 128, or the group's rows rounded up to 16 for the packed tiles of
+// a replayed kernel-tile store), ends go to the caller's outputs.  MODE 1 (proxy): columns 85c + r are
 // Cartesian component c of proxy r, ends go to the unit's partial rows `part`.
 // MODE 2 (upward): columns j < 128 are proxies row0 + j.
 //
 // FP16 leaf pass (scaled, the same in every lane): the chain's operands were
-// scaled by powers of two, the weight rows of field f by 1 / fsc and the
-// kernel tile's column of target t by 1 / csc[tgt + t] (csc null: DOWN
-// chains, unscaled columns); the fold multiplies the chain by fsc * csc
-// first (exact: powers of two).
+// scaled by powers of two, the weight rows of field f by 1 / fsc and (kernel
+// chains) the kernel tile's column of target t by tscale[tgt + t] (DOWN
+// chains: unscaled columns).  The running sums are kept in the columns'
+// scaled domain: a kernel chain adds chain x fsc, a DOWN chain chain x fsc x
+// tscale, and the group's end multiplies by tinv = 1 / tscale.  Powers of two
+// commute with rounding, so this gives the unscaled sums' bits while kernel
+// chains (all but one or a few per group) need no per-column factors.
+// Several warps of one lane quarter can share a fold: warp part_i of nparts
+// takes chunks part_i, part_i + nparts, ... (pairs of chunks mid-group).
 template <int MODE>
 __device__ __noinline__ void fold_chain(uint32_t td, int q, int lane, bool end, bool first, int tgt, int nt,
                                         const int32_t *__restrict__ perm, double *out_x, double *out_y,
                                         int64_t ld_out, int f0, int nf, bool skip, float *part, bool scaled = false,
-                                        float fsc = 1.f, const float *__restrict__ csc = nullptr) {
+                                        float fsc = 1.f, bool down = false, const float *__restrict__ tscale = nullptr,
+                                        const float *__restrict__ tinv = nullptr, int half = 128, int part_i = 0,
+                                        int nparts = 1) {
     const int f = 16 * q + (lane & 15), odd = lane >> 4;
-    float cs4[4] = {1.f, 1.f, 1.f, 1.f};   // column scale of target slot 32k + lane
-    if (MODE == 0 && csc)
+    // per target slot 32k + lane: its scale (DOWN chains) and inverse (the end)
+    float csd[4] = {1.f, 1.f, 1.f, 1.f}, cse[4] = {1.f, 1.f, 1.f, 1.f};
+    if (MODE == 0 && scaled && down)
 #pragma unroll
-        for (int k = 0; k < 4; ++k) cs4[k] = 32 * k + lane < nt ? csc[tgt + 32 * k + lane] : 1.f;
-    // this chain's scale undone on a 16-column chunk starting at column c
+        for (int k = 0; k < 4; ++k) csd[k] = 32 * k + lane < nt ? tscale[tgt + 32 * k + lane] : 1.f;
+    if (MODE == 0 && scaled && end)
+#pragma unroll
+        for (int k = 0; k < 4; ++k) cse[k] = 32 * k + lane < nt ? tinv[tgt + 32 * k + lane] : 1.f;
+    // x[m] *= v[column c + m] for a 16-column chunk starting at column c
+    auto colmul = [&](float (&x)[16], int c, const float (&v)[4]) {
+        const int b = c >= half ? c - half : c, k = b >> 5;
+        const float src = k == 0 ? v[0] : k == 1 ? v[1] : k == 2 ? v[2] : v[3];
+#pragma unroll
+        for (int m = 0; m < 16; ++m) x[m] *= __shfl_sync(0xffffffffu, src, (b & 31) + m);
+    };
+    // the chain into the running sums' domain
     auto unscale = [&](float (&x)[16], int c) {
         if (!scaled) return;
-        const int b = c & 127, k = b >> 5;
-        const float src = k == 0 ? cs4[0] : k == 1 ? cs4[1] : k == 2 ? cs4[2] : cs4[3];
 #pragma unroll
-        for (int m = 0; m < 16; ++m) x[m] *= fsc * __shfl_sync(0xffffffffu, src, (b & 31) + m);
+        for (int m = 0; m < 16; ++m) x[m] *= fsc;
+        if (down) colmul(x, c, csd);
     };
     int idx[4] = {0, 0, 0, 0};   // caller index of target slot 32k + lane
     if (MODE == 0 && end)
@@ -358,18 +407,18 @@ __device__ __noinline__ void fold_chain(uint32_t td, int q, int lane, bool end, 
     const bool wr = end && (MODE != 0 || f0 + f < nf) && !skip;
     double *ox = MODE == 0 ? out_x + (size_t)(f0 + f) * ld_out : nullptr;
     double *oy = MODE == 0 ? out_y + (size_t)(f0 + f) * ld_out : nullptr;
-    // chunks of 16 columns: leaf component ch = c / 128, target slots
-    // c % 128 ..+15 (at a group's end only the chunks that hold targets);
+    // chunks of 16 columns: leaf component ch = c / half, target slots
+    // c % half ..+15 (at a group's end only the chunks that hold targets);
     // proxy: all 16 chunks
-    const int per = (MODE != 1 && end) ? (nt + 15) / 16 : 8;
+    const int per = (MODE != 1 && end) ? (nt + 15) / 16 : (MODE == 0 ? half / 16 : 8);
     const int nchunk = MODE == 2 ? per : 2 * per;   // upward: one component, columns 0..127
-    auto col = [&](int i) { return (i / per) * 128 + (i % per) * 16; };
+    auto col = [&](int i) { return (i / per) * half + (i % per) * 16; };
     if (!end) {
         // mid-group: the MMA warp waits for this fold before its next chain,
         // so two chunks' loads are in flight per wait (nchunk is even here)
         float x0[16], x1[16], r0[16], r1[16];
 #pragma unroll 1
-        for (int i = 0; i < nchunk; i += 2) {
+        for (int i = 2 * part_i; i < nchunk; i += 2 * nparts) {
             const int c0 = col(i), c1 = col(i + 1);
             tmem_ld16(td + c0, x0);
             tmem_ld16(td + c1, x1);
@@ -395,7 +444,7 @@ __device__ __noinline__ void fold_chain(uint32_t td, int q, int lane, bool end, 
     }
     float x[16], r[16];
 #pragma unroll 1
-    for (int i = 0; i < nchunk; ++i) {
+    for (int i = part_i; i < nchunk; i += nparts) {
         const int c = col(i);
         tmem_ld16(td + c, x);
         if (!first) tmem_ld16(td + 256 + c, r);
@@ -405,22 +454,83 @@ __device__ __noinline__ void fold_chain(uint32_t td, int q, int lane, bool end, 
 #pragma unroll
             for (int m = 0; m < 16; ++m) x[m] += r[m];
         }
-        const int ik = (c & 127) >> 5;
+        if (MODE == 0 && scaled) colmul(x, c, cse);   // out of the columns' scaled domain
+        const int ik = (c >= half ? c - half : c) >> 5;
         const int idk = ik == 0 ? idx[0] : ik == 1 ? idx[1] : ik == 2 ? idx[2] : idx[3];
-        emit_chunk<MODE>(x, c, f, odd, nt, idk, c < 128 ? ox : oy, wr, part);
+        emit_chunk<MODE>(x, c, f, odd, nt, idk, c < half ? ox : oy, wr, part, half);
     }
 }
+
+// Outputs of target t of a leaf group without sources: its self pair alone.
+__device__ __noinline__ void self_only(const TcArgs &a, const MixGroup &G, int t) {
+    const int pos = G.tgt + t, idx = a.perm[pos];
+    const double2 sk = a.selfk[pos];
+    for (int f = 0; f < kF && a.f0 + f < a.nf; ++f) {
+        const double w = (double)a.wF[(size_t)pos * kF + f];
+        a.out_x[(size_t)(a.f0 + f) * a.ld_out + idx] = sk.x * w;
+        a.out_y[(size_t)(a.f0 + f) * a.ld_out + idx] = sk.y * w;
+    }
+}
+
+// A warp's window on a group's item records, 32 at a time: lane i holds
+// record k0 + i, and the next 32 are loaded one batch ahead, so a warp that
+// walks items faster than a global load returns (the MMA, loader and fold
+// warps) does not wait on one load per item.  k must be warp-uniform and
+// non-decreasing.
+struct ItemWindow {
+    const TcItem *items;
+    int k0, ie;
+    TcItem cur, nxt;
+    __device__ __forceinline__ void start(const TcItem *it, int ib, int e, int lane) {
+        items = it;
+        k0 = ib;
+        ie = e;
+        cur = ib + lane < e ? it[ib + lane] : TcItem{};
+        nxt = ib + 32 + lane < e ? it[ib + 32 + lane] : TcItem{};
+    }
+    __device__ __forceinline__ void seek(int k, int lane) {
+        while (k >= k0 + 32) {
+            cur = nxt;
+            k0 += 32;
+            nxt = k0 + 32 + lane < ie ? items[k0 + 32 + lane] : TcItem{};
+        }
+    }
+    __device__ __forceinline__ TcItem get(int k, int lane) {
+        seek(k, lane);
+        const int l = k - k0;
+        TcItem r;
+        r.off = __shfl_sync(0xffffffffu, cur.off, l);
+        r.cnt = __shfl_sync(0xffffffffu, cur.cnt, l);
+        r.kb = __shfl_sync(0xffffffffu, cur.kb, l);
+        r.kind = __shfl_sync(0xffffffffu, cur.kind, l);
+        r.dx = __shfl_sync(0xffffffffu, cur.dx, l);
+        r.dy = __shfl_sync(0xffffffffu, cur.dy, l);
+        r.dz = __shfl_sync(0xffffffffu, cur.dz, l);
+        r.row0 = __shfl_sync(0xffffffffu, cur.row0, l);
+        return r;
+    }
+    __device__ __forceinline__ int kind(int k, int lane) {
+        seek(k, lane);
+        return __shfl_sync(0xffffffffu, cur.kind, k - k0);
+    }
+};
 
 // JOINT: one launch over the groups of several grids (of one degree): group
 // gi belongs to the grid k with J.beg[k] <= gi < J.beg[k + 1] and carries
 // that grid's arguments.  Otherwise J.g[0] is the only grid.
-template <int MODE, bool JOINT, bool F16>
+// TS (FP16 leaf pass, one grid): 0 the producers compute the kernel tiles;
+// 1 they compute them and also record them in the grid's kernel-tile store;
+// 2 the loader copies them from the store into the kernel-tile ring and the
+// producers only write the outputs of groups without sources.
+template <int MODE, bool JOINT, bool F16, int TS = 0>
 __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(const __grid_constant__ TcJoint J, int *err) {
     static_assert(!F16 || MODE == 0, "FP16 operands in the leaf pass only");
+    static_assert(TS == 0 || (MODE == 0 && F16 && !JOINT), "kernel-tile store: FP16 leaf pass of one grid");
     constexpr int SK = F16 ? kStageKF16 : kStageK;   // sources per stage
     constexpr int SU = SK / 8;                        // store units (8 sources) per stage
     extern __shared__ __align__(1024) unsigned char smem_raw[];
-    TcSmem &sm = *reinterpret_cast<TcSmem *>(smem_raw);
+    constexpr int KS = TcSmem<TS>::KS, WS = TcSmem<TS>::WS;
+    TcSmem<TS> &sm = *reinterpret_cast<TcSmem<TS> *>(smem_raw);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int n = J.g[0].d + 1, P = J.g[0].P;
     const int total = JOINT ? J.beg[J.ngrids] : J.g[0].ngroups;
@@ -442,24 +552,33 @@ __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(const __grid_const
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
     if (tid == 0) {
-        for (int j = 0; j < kKStages; ++j) {
-            dev::mbar_init(&sm.kfull[j], kProdWarps);
+        for (int j = 0; j < KS; ++j) {
+            // replay: the loader's arrival and its copies' bytes fill a stage
+            dev::mbar_init(&sm.kfull[j], TS == 2 ? 1 : kProdWarps);
             dev::mbar_init(&sm.kempty[j], 1);
         }
-        for (int j = 0; j < kWStages; ++j) {
+        for (int j = 0; j < WS; ++j) {
             dev::mbar_init(&sm.wfull[j], 1);
             dev::mbar_init(&sm.wempty[j], 1);
         }
         dev::mbar_init(&sm.accfull, 1);
-        dev::mbar_init(&sm.accfree, kFoldWarps);
+        // replay: the idle producer warps fold too, three warps per lane quarter
+        dev::mbar_init(&sm.accfree, TS == 2 ? kFoldWarps + kProdWarps : kFoldWarps);
         dev::mbar_init(&sm.fin, 1);
         dev::fence_mbar_init();
         sm.abort = 0;
     }
-    for (int k = tid; k < kKmap; k += kThreads) {
+    for (int k = tid; TS != 2 && k < kKmap; k += kThreads) {
         const int kk = k < 3 * P ? k : 0;
         const int p = kk / 3;
         sm.kmap[k] = (p % n) | ((p / n) << 8) | ((kk % 3) << 16);
+    }
+    if (TS == 2) {
+        // replay copies only a group's rows: the ring's other rows hold
+        // zeros or an earlier group's finite values (columns no output reads)
+        uint4 *z = reinterpret_cast<uint4 *>(sm.ring);
+        for (int i = tid; i < (int)(sizeof(sm.ring) / sizeof(uint4)); i += kThreads) z[i] = make_uint4(0u, 0u, 0u, 0u);
+        dev::fence_proxy_async();
     }
     tc_fence_before();
     __syncthreads();
@@ -467,7 +586,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(const __grid_const
     const uint32_t tmem = sm.tmem_base;
     uint32_t st = 0;   // stages this CTA has gone through
 
-    if (warp < kProdWarps) {
+    if (TS != 2 && warp < kProdWarps) {
         // ============================================================ producers
         // A stage's tasks are (row block of 32 targets, unit) pairs, one
         // 8-source unit of 32 rows each (a TF32 stage has 4 units, an FP16
@@ -479,7 +598,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(const __grid_const
         //   1 row block:    warp w takes unit w (TF32: warps 4-7 only arrive)
         // The source coordinates of a stage's k-steps (x[8] y[8] z[8] each,
         // relative to their panel's centre) arrive in shared memory with the
-        // stage's weights: the loader warp copies them up to kWStages stages
+        // stage's weights: the loader warp copies them up to WS stages
         // ahead, so no global-memory latency sits in a producer task.
 
         for (int gi = blockIdx.x; gi < total; gi += gridDim.x) {
@@ -527,15 +646,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(const __grid_const
             }
             if (ni == 0) {
                 // no sources: the self pair alone (thread t: target t)
-                if (MODE == 0 && tid < G.nt && !*abort) {
-                    const int pos = G.tgt + tid, idx = a.perm[pos];
-                    const double2 sk = a.selfk[pos];
-                    for (int f = 0; f < kF && a.f0 + f < a.nf; ++f) {
-                        const double w = (double)a.wF[(size_t)pos * kF + f];
-                        a.out_x[(size_t)(a.f0 + f) * a.ld_out + idx] = sk.x * w;
-                        a.out_y[(size_t)(a.f0 + f) * a.ld_out + idx] = sk.y * w;
-                    }
-                }
+                if (MODE == 0 && tid < G.nt && !*abort) self_only(a, G, tid);
                 continue;
             }
             // the kernel values' projections; FP16: with the row's scale in them
@@ -550,6 +661,12 @@ __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(const __grid_const
                 self_e = (float)sk.x * tsc;
                 self_n = (float)sk.y * tsc;
             }
+            // record: the group's tiles in the store, stage after stage; per
+            // MMA step four chunks (hi, lo x east, north) of the group's rows
+            // rounded up to 16, each the bytes of the ring's rows
+            const int nr16 = (G.nt + 15) & ~15;
+            const size_t cb = (size_t)nr16 * 32;
+            unsigned char *gtile = TS == 1 ? a.ktile + a.ktile_off[gi - J.beg[gk]] : nullptr;
             // item records are read one item ahead, so their latency hides
             // behind the current item's stages
             TcItem nxt = a.items[G.ib];
@@ -578,16 +695,16 @@ __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(const __grid_const
                 // self pairs (one test per item, the same for every thread)
                 const bool self_item = MODE == 0 && kind == 0 && it.off < G.tgt + G.nt && G.tgt < it.off + it.cnt;
                 for (int j = 0; j < nst; ++j, ++st) {
-                    const uint32_t slot = st % kKStages, kpar = ((st / kKStages) - 1) & 1;
+                    const uint32_t slot = st % KS, kpar = ((st / KS) - 1) & 1;
                     const int nks = (min(SK, it.cnt - SK * j) + 7) >> 3;   // k-steps of this stage
                     // the MMAs that last read this slot must be done before
                     // the first store into it
-                    bool slot_free = st < (uint32_t)kKStages;
+                    bool slot_free = st < (uint32_t)KS;
                     // the stage's upward factors (MODE 2) or source
                     // coordinates (point and proxy sources) are in aux
                     if ((MODE == 2 || kind != 2) && active && kfirst < nks)
-                        wait_bounded(&sm.wfull[st % kWStages], (st / kWStages) & 1, abort, err);
-                    const float4 *crd = reinterpret_cast<const float4 *>(sm.aux[st % kWStages]);
+                        wait_bounded(&sm.wfull[st % WS], (st / WS) & 1, abort, err);
+                    const float4 *crd = reinterpret_cast<const float4 *>(sm.aux[st % WS]);
                     // one task: the kernel-tile values of k-step kk for this
                     // lane's row (east / north, or the three Cartesian
                     // components in the proxy pass)
@@ -595,7 +712,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(const __grid_const
                             if (MODE == 2) {
                                 // upward: the BLI basis of proxy (i, j) at the 8 points,
                                 // F_i(xi) G_j(eta) from the per-point factors
-                                const float *Fb = sm.aux[st % kWStages] + 16 * n * kk;
+                                const float *Fb = sm.aux[st % WS] + 16 * n * kk;
                                 const float4 f0 = *reinterpret_cast<const float4 *>(Fb + 8 * up_i);
                                 const float4 f1 = *reinterpret_cast<const float4 *>(Fb + 8 * up_i + 4);
                                 const float4 g0 = *reinterpret_cast<const float4 *>(Fb + 8 * n + 8 * up_j);
@@ -676,8 +793,8 @@ __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(const __grid_const
                             if constexpr (F16) {
                                 // FP16 hi + lo: unit kk is K half kk & 1 of MMA step kk / 2,
                                 // the row's 8 values one 16-byte core-matrix row
-                                char *th = reinterpret_cast<char *>(sm.Kt[slot][kk >> 1][0]);
-                                char *tlo = reinterpret_cast<char *>(sm.Kt[slot][kk >> 1][1]);
+                                char *th = reinterpret_cast<char *>(sm.Kt(slot, kk >> 1, 0));
+                                char *tlo = reinterpret_cast<char *>(sm.Kt(slot, kk >> 1, 1));
                                 const int hb = 128 * (kk & 1);
                                 uint4 eh, el, nh, nl;
                                 split_f16x2(ve[0], ve[1], eh.x, el.x);
@@ -692,10 +809,17 @@ __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(const __grid_const
                                 *reinterpret_cast<uint4 *>(tlo + oe16 + hb) = el;
                                 *reinterpret_cast<uint4 *>(th + on16 + hb) = nh;
                                 *reinterpret_cast<uint4 *>(tlo + on16 + hb) = nl;
+                                if (TS == 1 && row < nr16) {
+                                    unsigned char *g = gtile + (size_t)(kk >> 1) * 4 * cb + oe16 + hb;
+                                    *reinterpret_cast<uint4 *>(g) = eh;
+                                    *reinterpret_cast<uint4 *>(g + cb) = nh;
+                                    *reinterpret_cast<uint4 *>(g + 2 * cb) = el;
+                                    *reinterpret_cast<uint4 *>(g + 3 * cb) = nl;
+                                }
                                 return;
                             }
                             // TF32 hi + lo (the tensor cores read lo's top 11 bits)
-                            float *th = sm.Kt[slot][kk][0], *tlo = sm.Kt[slot][kk][1];
+                            float *th = sm.Kt(slot, kk, 0), *tlo = sm.Kt(slot, kk, 1);
 #pragma unroll
                             for (int hh = 0; hh < 2; ++hh) {
                                 const float4 eh = make_float4(tf32_hi(ve[4 * hh]), tf32_hi(ve[4 * hh + 1]),
@@ -765,6 +889,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(const __grid_const
                     }
                     __syncwarp();
                     if (lane == 0) mbar_arrive(&sm.kfull[slot]);
+                    if (TS == 1) gtile += (size_t)4 * ((nks + 1) >> 1) * cb;
                 }
             }
         }
@@ -776,15 +901,18 @@ __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(const __grid_const
             const int gk = grid_of(gi);
             const TcArgs &a = J.g[gk];
             const MixGroup G = a.groups[gi - J.beg[gk]];
-            TcItem nxt = G.ib < G.ie ? a.items[G.ib] : TcItem{};
+            ItemWindow w;
+            w.start(a.items, G.ib, G.ie, lane);
+            // replay: bytes of one packed tile (east rows, then north rows)
+            const uint32_t ptile = 2u * (uint32_t)((G.nt + 15) & ~15) * 32u;
             for (int k = G.ib; k < G.ie; ++k) {
-                const TcItem it = nxt;
-                if (k + 1 < G.ie) nxt = a.items[k + 1];
+                const TcItem it = w.get(k, lane);
                 const int nst = (it.cnt + SK - 1) / SK;
                 for (int j = 0; j < nst; ++j, ++st) {
-                    const uint32_t slot = st % kKStages, jb = st % kWStages;
-                    wait_bounded(&sm.wfull[jb], (st / kWStages) & 1, abort, err);
-                    wait_bounded(&sm.kfull[slot], (st / kKStages) & 1, abort, err);
+                    const uint32_t slot = st % KS, jb = st % WS;
+                    // replay: the stage's one barrier covers its weight and kernel tiles
+                    if (TS != 2) wait_bounded(&sm.wfull[jb], (st / WS) & 1, abort, err);
+                    wait_bounded(&sm.kfull[slot], (st / KS) & 1, abort, err);
                     // a new chain overwrites the accumulator, whose last chain
                     // (cc - 1) the fold warps must have read
                     if (!chain_open && cc >= 1) wait_bounded(&sm.accfree, (cc - 1) & 1, abort, err);
@@ -792,25 +920,35 @@ __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(const __grid_const
                     if (lane == 0) {
                         if (!*abort) {
                             const int nks = (min(SK, it.cnt - SK * j) + 7) >> 3;
-                            if constexpr (F16) {
+                            if constexpr (TS == 2) {
+                                // packed tiles of MMA step s: hi at (2s) ptile, lo at (2s + 1) ptile
+                                const unsigned char *tb = sm.ring + sm.toff[slot];
+                                const unsigned char *wb = sm.ring + TcSmem<TS>::kKtBytes + sm.woff[slot];
+                                for (int s = 0; 2 * s < nks; ++s) {
+                                    const uint64_t aw = smem_desc_w16(wb + s * 2 * kW16UnitBytes);
+                                    const uint64_t bh = smem_desc(tb + 2 * s * ptile), bl = smem_desc(tb + (2 * s + 1) * ptile);
+                                    mma_ss_f16(tmem, aw, bh, (chain_open || s > 0) ? 1u : 0u);
+                                    mma_ss_f16(tmem, aw, bl, 1u);
+                                }
+                            } else if constexpr (F16) {
                                 // 16 sources per MMA: weight units 2s and 2s + 1
                                 for (int s = 0; 2 * s < nks; ++s) {
-                                    const uint64_t aw = smem_desc_w16(&sm.Wt[jb][s * (2 * kW16UnitBytes / 4)]);
-                                    const uint64_t bh = smem_desc(sm.Kt[slot][s][0]), bl = smem_desc(sm.Kt[slot][s][1]);
+                                    const uint64_t aw = smem_desc_w16(sm.Wt(jb) + s * (2 * kW16UnitBytes / 4));
+                                    const uint64_t bh = smem_desc(sm.Kt(slot, s, 0)), bl = smem_desc(sm.Kt(slot, s, 1));
                                     mma_ss_f16(tmem, aw, bh, (chain_open || s > 0) ? 1u : 0u);
                                     mma_ss_f16(tmem, aw, bl, 1u);
                                 }
                             } else {
                                 for (int s = 0; s < nks; ++s) {
-                                    const uint64_t aw = smem_desc(&sm.Wt[jb][s * kWStepFloats]);
-                                    const uint64_t bh = smem_desc(sm.Kt[slot][s][0]), bl = smem_desc(sm.Kt[slot][s][1]);
+                                    const uint64_t aw = smem_desc(sm.Wt(jb) + s * kWStepFloats);
+                                    const uint64_t bh = smem_desc(sm.Kt(slot, s, 0)), bl = smem_desc(sm.Kt(slot, s, 1));
                                     mma_ss(tmem, aw, bh, (chain_open || s > 0) ? 1u : 0u);
                                     mma_ss(tmem, aw, bl, 1u);
                                 }
                             }
                         }
                         mma_commit(&sm.kempty[slot]);
-                        mma_commit(&sm.wempty[jb]);
+                        if (TS != 2) mma_commit(&sm.wempty[jb]);
                     }
                     chain_open = true;
                     __syncwarp();
@@ -831,15 +969,23 @@ __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(const __grid_const
         __syncwarp();
     } else if (warp == kLoadWarp) {
         // ============================================================ loads
+        // replay: ring heads, the oldest stage still in flight
+        uint32_t thead = 0, whead = 0, oldest = 0;
         for (int gi = blockIdx.x; gi < total; gi += gridDim.x) {
             const int gk = grid_of(gi);
             const TcArgs &a = J.g[gk];
             const MixGroup G = a.groups[gi - J.beg[gk]];
-            TcItem nxt = G.ib < G.ie ? a.items[G.ib] : TcItem{};
+            ItemWindow w;
+            w.start(a.items, G.ib, G.ie, lane);
+            // replay: the group's recorded tiles, stage after stage (per MMA
+            // step, hi then lo, each the group's east rows then its north
+            // rows, rounded up to 16 rows of 32 bytes)
+            const unsigned char *tsrc = TS == 2 ? a.ktile + a.ktile_off[gi - J.beg[gk]] : nullptr;
+            const uint32_t cb = (uint32_t)((G.nt + 15) & ~15) * 32u;
             for (int k = G.ib; k < G.ie; ++k) {
-                const TcItem it = nxt;
+                const TcItem it = w.get(k, lane);
                 if (k + 1 < G.ie) {
-                    nxt = a.items[k + 1];
+                    const TcItem nxt = w.get(k + 1, lane);
                     // the next item's weight tiles (and source coordinates)
                     // into L2 while this item's stages run
                     if (lane == 0 && MODE != 2) {
@@ -849,67 +995,122 @@ __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(const __grid_const
                                         ((nks + 1) & ~1u) * kW16UnitBytes);
                         else
                             prefetch_l2(a.bstore + (size_t)nxt.kb * kWStepFloats, nks * kWStepFloats * 4u);
-                        if ((nxt.kind & 3) != 2) prefetch_l2(a.sxyz + (size_t)nxt.kb * 24, nks * 96u);
+                        if (TS != 2 && (nxt.kind & 3) != 2) prefetch_l2(a.sxyz + (size_t)nxt.kb * 24, nks * 96u);
                     }
                 }
                 const int nst = (it.cnt + SK - 1) / SK;
                 for (int j = 0; j < nst; ++j, ++st) {
-                    const uint32_t jb = st % kWStages, ub = st / kWStages;
-                    if (ub > 0) wait_bounded(&sm.wempty[jb], (ub - 1) & 1, abort, err);
-                    if (lane == 0) {
-                        const int ncol = min(SK, it.cnt - SK * j), nks = (ncol + 7) >> 3;
-                        // FP16: whole 16-source MMA steps (the store has a spare unit at its end)
-                        const uint32_t wbytes = F16 ? (uint32_t)((nks + 1) & ~1) * kW16UnitBytes
-                                                    : (uint32_t)nks * kWStepFloats * 4;
-                        // with the weights: the stage's BLI factors (upward) or
-                        // its point / proxy sources' coordinates (24 floats per
-                        // k-step; DOWN rows need none)
-                        const uint32_t lbytes = MODE == 2 ? (uint32_t)nks * 64 * n
-                                                : (it.kind & 3) != 2 ? (uint32_t)nks * 96u : 0u;
-                        dev::mbar_expect_tx(&sm.wfull[jb], wbytes + lbytes);
-                        if (!*abort) {
-                            if (lbytes)
-                                dev::bulk_g2s(sm.aux[jb],
-                                              MODE == 2 ? (const void *)(a.basis + (size_t)(it.row0 + SU * j) * 16 * n)
-                                                        : (const void *)(a.sxyz + (size_t)(it.kb + SU * j) * 24),
-                                              lbytes, &sm.wfull[jb]);
-                            const void *wsrc =
-                                F16 ? static_cast<const void *>(static_cast<const char *>(a.bstore16) +
-                                                                (size_t)(it.kb + SU * j) * kW16UnitBytes)
-                                    : static_cast<const void *>(a.bstore + (size_t)(it.kb + SU * j) * kWStepFloats);
-                            dev::bulk_g2s(sm.Wt[jb], wsrc, wbytes, &sm.wfull[jb]);
+                    const int nks = (min(SK, it.cnt - SK * j) + 7) >> 3;
+                    if constexpr (TS == 2) {
+                        // the stage's kernel tiles and weight tiles, each one
+                        // bulk copy into its ring (from the start of a ring
+                        // when they do not fit before its end), once the stage
+                        // slot and both ranges are free: stages retire in order
+                        const uint32_t nsteps = (uint32_t)(nks + 1) >> 1;
+                        const uint32_t sb = nsteps * 4u * cb, wb = nsteps * 2u * kW16UnitBytes;
+                        const uint32_t tpos = thead + sb > (uint32_t)kTRingBytes ? 0u : thead;
+                        const uint32_t wpos = whead + wb > (uint32_t)kWRingBytes ? 0u : whead;
+                        while (oldest < st) {
+                            bool clash = st - oldest >= (uint32_t)KS;
+                            for (uint32_t x = oldest; !clash && x < st; ++x) {
+                                const uint32_t xs = x % KS;
+                                const uint32_t t0 = sm.toff[xs], t1 = t0 + sm.tlen[xs];
+                                const uint32_t w0 = sm.woff[xs], w1 = w0 + sm.wlen[xs];
+                                clash = (tpos < t1 && t0 < tpos + sb) || (wpos < w1 && w0 < wpos + wb);
+                            }
+                            if (!clash) break;
+                            wait_bounded(&sm.kempty[oldest % KS], (oldest / KS) & 1, abort, err);
+                            ++oldest;
                         }
+                        const uint32_t slot = st % KS;
+                        if (lane == 0) {
+                            sm.toff[slot] = tpos;
+                            sm.tlen[slot] = sb;
+                            sm.woff[slot] = wpos;
+                            sm.wlen[slot] = wb;
+                            // the offsets are written before the arrival the MMA warp waits on
+                            dev::mbar_expect_tx(&sm.kfull[slot], sb + wb);
+                            if (!*abort) {
+                                dev::bulk_g2s(sm.ring + tpos, tsrc, sb, &sm.kfull[slot]);
+                                dev::bulk_g2s(sm.ring + TcSmem<TS>::kKtBytes + wpos,
+                                              static_cast<const char *>(a.bstore16) + (size_t)(it.kb + SU * j) * kW16UnitBytes,
+                                              wb, &sm.kfull[slot]);
+                            }
+                        }
+                        __syncwarp();
+                        tsrc += sb;
+                        thead = tpos + sb;
+                        whead = wpos + wb;
+                    } else {
+                        const uint32_t jb = st % WS, ub = st / WS;
+                        if (ub > 0) wait_bounded(&sm.wempty[jb], (ub - 1) & 1, abort, err);
+                        if (lane == 0) {
+                            // FP16: whole 16-source MMA steps (the store has a spare unit at its end)
+                            const uint32_t wbytes = F16 ? (uint32_t)((nks + 1) & ~1) * kW16UnitBytes
+                                                        : (uint32_t)nks * kWStepFloats * 4;
+                            // with the weights: the stage's BLI factors (upward) or
+                            // its point / proxy sources' coordinates (24 floats per
+                            // k-step; DOWN rows need none)
+                            const uint32_t lbytes = MODE == 2 ? (uint32_t)nks * 64 * n
+                                                    : (it.kind & 3) != 2 ? (uint32_t)nks * 96u : 0u;
+                            dev::mbar_expect_tx(&sm.wfull[jb], wbytes + lbytes);
+                            if (!*abort) {
+                                if (lbytes)
+                                    dev::bulk_g2s(sm.aux[jb],
+                                                  MODE == 2 ? (const void *)(a.basis + (size_t)(it.row0 + SU * j) * 16 * n)
+                                                            : (const void *)(a.sxyz + (size_t)(it.kb + SU * j) * 24),
+                                                  lbytes, &sm.wfull[jb]);
+                                const void *wsrc =
+                                    F16 ? static_cast<const void *>(static_cast<const char *>(a.bstore16) +
+                                                                    (size_t)(it.kb + SU * j) * kW16UnitBytes)
+                                        : static_cast<const void *>(a.bstore + (size_t)(it.kb + SU * j) * kWStepFloats);
+                                dev::bulk_g2s(sm.Wt(jb), wsrc, wbytes, &sm.wfull[jb]);
+                            }
+                        }
+                        __syncwarp();
                     }
-                    __syncwarp();
                 }
             }
         }
         // no bulk copy may still be landing when the CTA exits
-        if (lane == 0)
-            for (uint32_t j = 0; j < (uint32_t)kWStages && j < st; ++j) {
-                const uint32_t uses = (st - 1 - j) / kWStages + 1;
+        if (TS == 2 && lane == 0)
+            for (uint32_t x = oldest; x < st; ++x) wait_drain(&sm.kfull[x % KS], (x / KS) & 1, err);
+        if (TS != 2 && lane == 0)
+            for (uint32_t j = 0; j < (uint32_t)WS && j < st; ++j) {
+                const uint32_t uses = (st - 1 - j) / WS + 1;
                 wait_drain(&sm.wfull[j], (uses - 1) & 1, err);
             }
         __syncwarp();
     }
     else {
         // ============================================================ folds
+        // (replay: warps 0-7 and 10-13, fold part 0, 1 or 2 of their lane
+        // quarter warp % 4; otherwise warps 10-13)
         const int q = warp & 3;
         const uint32_t tq = tmem + ((uint32_t)(32 * q) << 16);
+        const int part_i = TS == 2 ? (warp < 4 ? 0 : warp < kProdWarps ? 1 : 2) : 0, nparts = TS == 2 ? 3 : 1;
         uint32_t cc = 0;   // chains folded
         for (int gi = blockIdx.x; gi < total; gi += gridDim.x) {
             const int gk = grid_of(gi);
             const TcArgs &a = J.g[gk];
             const MixGroup G = a.groups[gi - J.beg[gk]];
+            if (TS == 2 && G.ib == G.ie) {
+                // a group without sources: the self pairs, by warps 0-7
+                if (tid < G.nt && !*abort) self_only(a, G, tid);
+                continue;
+            }
             bool first = true;
+            ItemWindow w;
+            w.start(a.items, G.ib, G.ie, lane);
             for (int k = G.ib; k < G.ie; ++k) {
-                if (!(a.items[k].kind & kTcFlush)) continue;
+                const int kind = w.kind(k, lane);
+                if (!(kind & kTcFlush)) continue;
                 wait_bounded(&sm.accfull, cc & 1, abort, err);
                 tc_fence_after();
                 // FP16: the chain's weight rows are the fields' source weights
                 // (scaled per field) against scaled kernel columns, or their
                 // potentials (scaled per field) against unscaled DOWN columns
-                const bool down_chain = (a.items[k].kind & 3) == 2;
+                const bool down_chain = (kind & 3) == 2;
                 const float fsc = F16 ? 1.f / f16_scale(__uint_as_float(a.fmax[(down_chain ? kF : 0) + 16 * q + (lane & 15)]))
                                       : 1.f;
                 fold_chain<MODE>(tq, q, lane, k == G.ie - 1, first, G.tgt, G.nt,
@@ -917,7 +1118,8 @@ __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(const __grid_const
                                  MODE == 1   ? a.partial + ((size_t)G.out * P + G.row0) * 3 * kF
                                  : MODE == 2 ? a.partial + ((size_t)G.out * P + G.row0) * kF
                                              : nullptr,
-                                 F16, fsc, F16 && !down_chain ? a.tinv : nullptr);
+                                 F16, fsc, down_chain, a.tscale, a.tinv, TS == 2 ? (G.nt + 15) & ~15 : 128, part_i,
+                                 nparts);
                 tc_fence_before();
                 __syncwarp();
                 if (lane == 0) mbar_arrive(&sm.accfree);
@@ -1144,39 +1346,41 @@ __global__ void self_pair_kernel(const double4 *__restrict__ pool, int n, double
     selfk[p] = make_double2(sx / dev::kCons, sy / dev::kCons);
 }
 
-static_assert(sizeof(TcSmem) + 1024 <= 227 * 1024, "the leaf kernel's shared memory fits one SM");
+static_assert(tc_smem_need<0>() <= 227 * 1024 && tc_smem_need<2>() <= 227 * 1024,
+              "the leaf kernel's shared memory fits one SM");
 
-size_t tc_smem_bytes() {
-    // above half of the SM's shared memory: one CTA per SM, which owns all
-    // 512 tensor memory columns
-    const size_t need = sizeof(TcSmem) + 1024;
-    return need > 120 * 1024 ? need : 120 * 1024;
+// Dynamic shared memory of a launch: above half of the SM's, so one CTA per
+// SM, which owns all 512 tensor memory columns.
+template <int TS>
+static size_t tc_smem_launch() {
+    return tc_smem_need<TS>() > 120 * 1024 ? tc_smem_need<TS>() : 120 * 1024;
 }
+size_t tc_smem_bytes() { return tc_smem_launch<0>(); }
 
-template <int MODE, bool JOINT, bool F16 = false>
+template <int MODE, bool JOINT, bool F16 = false, int TS = 0>
 static void launch_tc(const TcJoint &J, int nsm, int cta_groups, int *err, cudaStream_t st) {
     const int total = J.beg[J.ngrids];
     if (total <= 0) return;
-    const size_t smem = tc_smem_bytes();
+    const size_t smem = tc_smem_launch<TS>();
     static std::atomic<unsigned long long> done{0};
-    smem_attr_once((const void *)tc_leaf_kernel<MODE, JOINT, F16>, (int)smem, done);
+    smem_attr_once((const void *)tc_leaf_kernel<MODE, JOINT, F16, TS>, (int)smem, done);
     // every SM busy, but no CTA longer than cta_groups groups: with short
     // CTAs, kernels of other streams (higher-priority grids) get SMs as CTAs
     // retire
     const int per = cta_groups > 0 ? cta_groups : 1;
     int grid = (total + per - 1) / per;
     if (grid < nsm) grid = total < nsm ? total : nsm;
-    tc_leaf_kernel<MODE, JOINT, F16><<<grid, kThreads, smem, st>>>(J, err);
+    tc_leaf_kernel<MODE, JOINT, F16, TS><<<grid, kThreads, smem, st>>>(J, err);
 }
 
-template <int MODE, bool F16 = false>
+template <int MODE, bool F16 = false, int TS = 0>
 static void launch_tc(const TcArgs &a, int nsm, int cta_groups, int *err, cudaStream_t st) {
     TcJoint J{};
     J.g[0] = a;
     J.ngrids = 1;
     J.beg[0] = 0;
     J.beg[1] = a.ngroups;
-    launch_tc<MODE, false, F16>(J, nsm, cta_groups, err, st);
+    launch_tc<MODE, false, F16, TS>(J, nsm, cta_groups, err, st);
 }
 
 void launch_tc_leaf_joint(const TcArgs *grids, int ngrids, int nsm, int cta_groups, int *err, cudaStream_t st) {
@@ -1194,8 +1398,12 @@ void launch_tc_leaf_joint(const TcArgs *grids, int ngrids, int nsm, int cta_grou
         launch_tc<0, true, false>(J, nsm, cta_groups, err, st);
 }
 
-void launch_tc_leaf(const TcArgs &a, int nsm, int cg, int *err, cudaStream_t st) {
-    if (a.bstore16)
+void launch_tc_leaf(const TcArgs &a, int nsm, int cg, int *err, cudaStream_t st, int tiles) {
+    if (a.bstore16 && a.ktile && tiles == 1)
+        launch_tc<0, true, 1>(a, nsm, cg, err, st);
+    else if (a.bstore16 && a.ktile && tiles == 2)
+        launch_tc<0, true, 2>(a, nsm, cg, err, st);
+    else if (a.bstore16)
         launch_tc<0, true>(a, nsm, cg, err, st);
     else
         launch_tc<0, false>(a, nsm, cg, err, st);

@@ -70,6 +70,7 @@ class GridStats(C.Structure):
         ("macs_up", C.c_double), ("macs_down", C.c_double),
         ("device_bytes", C.c_int64), ("setup_seconds", C.c_double), ("mixed_bytes", C.c_int64),
         ("macs_up_batched", C.c_double), ("macs_down_batched", C.c_double), ("launches_batched", C.c_int64),
+        ("tile_store_bytes", C.c_int64),
     ]
 
 
@@ -78,7 +79,7 @@ class Tune(C.Structure):
     _fields_ = [
         ("chain_ksteps", C.c_int32), ("tree_passes", C.c_int32), ("up_chunk", C.c_int32),
         ("proxy_unit_kpairs", C.c_int32), ("cta_groups", C.c_int32), ("field_block", C.c_int32),
-        ("f16", C.c_int32),
+        ("f16", C.c_int32), ("tile_store", C.c_int32),
     ]
 
     def as_dict(self):

@@ -354,3 +354,55 @@ def test_f16_batch_invariance_and_zero_field():
         ox, oy = grid.solve(ssh[f:f + 1], form=S.FORM_MIXED)
         torch.cuda.synchronize()
         assert torch.equal(ox[0], bx[f]) and torch.equal(oy[0], by[f])
+
+
+@pytest.mark.parametrize("degree,tree", [(8, 1), (8, 0), (10, 1)])
+def test_tile_store_records_and_replays_bitwise(degree, tree):
+    """sal_tune.tile_store = 1: the first FP16 leaf pass records its kernel
+    tiles (near-field, proxy and DOWN rows) in device memory and later solves
+    replay them.  The recording solve, the replays (other fields, fewer fields,
+    graphs on a stream) and the solve after switching the store off again all
+    equal the computing leaf pass bit for bit; the memory estimate counts the
+    store, whose size the stats report."""
+    torch = _torch()
+    S, g, hs, grid = _grid("small_20000", 60, 6, seed=23, degree=degree, max_fields=64)
+    hs = hs * np.array([1.0, 1e-3, 1e3, 1e-6, 0.0, 5.0])[:, None]
+    ssh = torch.tensor(hs, device="cuda")
+    grid.tune(tree_passes=tree, f16=1, tile_store=0)
+    ref = [v.clone() for v in grid.solve(ssh, form=S.FORM_MIXED)]
+    ref3 = [v.clone() for v in grid.solve(ssh[2:5], form=S.FORM_MIXED)]
+    torch.cuda.synchronize()
+    tile_bytes = grid.stats()["tile_store_bytes"]
+    assert tile_bytes > 0
+    grid.tune(tile_store=1)
+    assert grid.tune()["tile_store"] == 1
+    est = grid.stats()["mixed_bytes"]
+    before = grid.stats()["device_bytes"]
+    for k in range(3):   # record, then replays
+        ox, oy = grid.solve(ssh, form=S.FORM_MIXED)
+        torch.cuda.synchronize()
+        assert torch.equal(ox, ref[0]) and torch.equal(oy, ref[1]), k
+    assert grid.stats()["device_bytes"] - before == est
+    assert est > tile_bytes
+    ox, oy = grid.solve(ssh[2:5], form=S.FORM_MIXED)
+    torch.cuda.synchronize()
+    assert torch.equal(ox, ref3[0]) and torch.equal(oy, ref3[1])
+    # captured graphs replay the recorded tiles too
+    # (a call shape is captured on its second solve and launched as a graph
+    # from its third)
+    grid.set_graphs(True)
+    s = torch.cuda.Stream()
+    ox, oy = torch.empty_like(ssh), torch.empty_like(ssh)
+    for k in range(4):
+        with torch.cuda.stream(s):
+            ox.zero_()
+            oy.zero_()
+            grid.solve(ssh, form=S.FORM_MIXED, out=(ox, oy), stream=s.cuda_stream)
+        s.synchronize()
+        assert torch.equal(ox, ref[0]) and torch.equal(oy, ref[1]), k
+    grid.set_graphs(False)
+    grid.tune(tile_store=0)
+    ox, oy = grid.solve(ssh, form=S.FORM_MIXED)
+    torch.cuda.synchronize()
+    assert torch.equal(ox, ref[0]) and torch.equal(oy, ref[1])
+    grid.sync()
