@@ -1031,10 +1031,12 @@ __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(const __grid_const
                             // the offsets are written before the arrival the MMA warp waits on
                             dev::mbar_expect_tx(&sm.kfull[slot], sb + wb);
                             if (!*abort) {
-                                dev::bulk_g2s(sm.ring + tpos, tsrc, sb, &sm.kfull[slot]);
-                                dev::bulk_g2s(sm.ring + TcSmem<TS>::kKtBytes + wpos,
-                                              static_cast<const char *>(a.bstore16) + (size_t)(it.kb + SU * j) * kW16UnitBytes,
-                                              wb, &sm.kfull[slot]);
+                                // the tiles are read once per solve: they leave L2 first, to
+                                // the weight tiles, which other groups read again
+                                dev::bulk_g2s_hint(sm.ring + tpos, tsrc, sb, &sm.kfull[slot], dev::l2_evict_first());
+                                dev::bulk_g2s_hint(sm.ring + TcSmem<TS>::kKtBytes + wpos,
+                                                   static_cast<const char *>(a.bstore16) + (size_t)(it.kb + SU * j) * kW16UnitBytes,
+                                                   wb, &sm.kfull[slot], dev::l2_evict_last());
                             }
                         }
                         __syncwarp();
