@@ -485,6 +485,16 @@ def summarize(reqs: list, cells: dict, wall: float, batches: list | None = None)
                 d["batches"] = len(bs)
                 d["mean_fields_per_batch"] = float(np.mean([b[1] for b in bs]))
                 d["mean_batch_ms"] = float(np.mean([(b[3] - b[2]) * 1e3 for b in bs]))
+                d["max_batch_ms"] = float(max((b[3] - b[2]) * 1e3 for b in bs))
         per[name] = d
     out["per_grid"] = per
+    if batches:
+        # where the tail comes from: the longest stretch with no batch launched
+        # (a stalled host loop) against the longest batch (a slow device)
+        ls = sorted(b[2] for b in batches if b[2] >= t0)
+        if len(ls) > 1:
+            gaps = np.diff(ls)
+            k = int(np.argmax(gaps))
+            out["max_launch_gap_ms"] = float(gaps[k] * 1e3)
+            out["max_launch_gap_at_s"] = float(ls[k] - t0)
     return out
