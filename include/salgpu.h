@@ -167,7 +167,9 @@ typedef struct {
                                    DOWN interpolation rows, FP16 hi/lo, which depend on the grid alone) in device
                                    memory, sal_grid_stats.tile_store_bytes of it: the first solve records them, later
                                    solves read them instead of computing them, with the same results bit for bit.
-                                   Allocated with the batched buffers; ignored with f16 = 0 or 32-field blocks */
+                                   m > 1 keeps one item in m of each leaf group (about 1/m of the bytes); later
+                                   solves copy those and compute the others.  Allocated with the batched buffers;
+                                   ignored with f16 = 0 or 32-field blocks */
 } sal_tune;
 
 /* Flattens the tree and lists into device-resident arrays (once per grid). */

@@ -675,6 +675,7 @@ static mix::TcArgs leaf_args(GridImpl &g, double *ox, double *oy, int64_t ld_out
         t.fmax = g.fmax;
         t.ktile = g.ktile;
         t.ktile_off = g.ktile_off;
+        t.tile_every = g.plan.tc_opt.tile_store > 1 ? g.plan.tc_opt.tile_store : 1;
     }
     return t;
 }
@@ -794,8 +795,9 @@ static void solve_mixed_block(GridImpl &g, const double *ssh, int64_t ld_ssh, in
         // 64-field blocks: the leaf pass's weight rows, then the tcgen05 leaf pass
         leaf_store();
         // with a kernel-tile store: the first leaf pass records the tiles, the
-        // later ones (stream-ordered after it) replay them
-        const int tiles = g.ktile ? (g.tile_recorded ? 2 : 1) : 0;
+        // later ones (stream-ordered after it) replay them: all of them (2), or
+        // one item in tile_store beside the producers' (3)
+        const int tiles = g.ktile ? (!g.tile_recorded ? 1 : pl.tc_opt.tile_store > 1 ? 3 : 2) : 0;
         mix::launch_tc_leaf(leaf_args(g, ox, oy, ld_out, f0, nf), g.nsm, cg, g.err, st, tiles);
         if (tiles == 1) g.tile_recorded = true;
     } else {
@@ -977,7 +979,8 @@ static int apply_tune(GridImpl &g, const sal_tune &t) {
     o.proxy_unit_kpairs = t.proxy_unit_kpairs;
     o.cta_groups = t.cta_groups;
     o.f16 = t.f16 ? 1 : 0;
-    o.tile_store = t.tile_store ? 1 : 0;
+    if (t.tile_store < 0) return set_error(SAL_EINVAL, "tile_store must be >= 0");
+    o.tile_store = t.tile_store;
     const TcOptions &c = g.plan.tc_opt;
     const bool same_plan = o.chain_ksteps == c.chain_ksteps && o.tree_passes == c.tree_passes &&
                            o.up_chunk == c.up_chunk && o.proxy_unit_kpairs == c.proxy_unit_kpairs &&
@@ -990,6 +993,7 @@ static int apply_tune(GridImpl &g, const sal_tune &t) {
         if (o.tile_store != c.tile_store) {
             int rc = release_mixed(g);
             if (rc) return rc;
+            plan_tile_offsets(&g.plan, o.tile_store > 1 ? o.tile_store : 1);
         }
         g.plan.tc_opt.cta_groups = o.cta_groups;
         g.plan.tc_opt.tile_store = o.tile_store;
@@ -1004,6 +1008,7 @@ static int apply_tune(GridImpl &g, const sal_tune &t) {
     } else {
         g.plan.tc_opt.cta_groups = o.cta_groups;
         g.plan.tc_opt.tile_store = o.tile_store;
+        plan_tile_offsets(&g.plan, o.tile_store > 1 ? o.tile_store : 1);
     }
     if (t.field_block == 32 && !g.plan.mix_built) plan_build_mix(g.tree, &g.plan);
     return SAL_OK;

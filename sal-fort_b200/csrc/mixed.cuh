@@ -73,10 +73,12 @@ struct TcArgs {
     const void *bstore16;
     const float *tscale, *tinv;
     const unsigned *fmax;
-    // FP16 leaf pass with a kernel-tile store: the store and per group the
-    // byte offset of its tiles (ngroups + 1 entries)
+    // FP16 leaf pass with a kernel-tile store: the store, per group the byte
+    // offset of its tiles (ngroups + 1 entries), and which items it holds:
+    // items every-1, 2 every-1, ... of each group (all with every = 1)
     unsigned char *ktile;
     const int64_t *ktile_off;
+    int tile_every;
 };
 // cta_groups: groups one CTA walks at most (the grid has every SM busy
 // otherwise)
@@ -88,7 +90,8 @@ struct TcJoint {
     int32_t ngrids;
 };
 // tiles (FP16 leaf pass with a.ktile set): 0 computes the kernel tiles,
-// 1 computes them and records them in a.ktile, 2 replays them from a.ktile
+// 1 computes them and records the stored items' in a.ktile, 2 replays them
+// all from a.ktile, 3 replays the stored items' and computes the others
 void launch_tc_leaf(const TcArgs &a, int nsm, int cta_groups, int *err, cudaStream_t st, int tiles = 0);
 void launch_tc_leaf_joint(const TcArgs *grids, int ngrids, int nsm, int cta_groups, int *err, cudaStream_t st);
 void launch_tc_proxy(const TcArgs &a, int nsm, int cta_groups, int *err, cudaStream_t st);

@@ -402,6 +402,24 @@ void plan_build_mix(const Tree &t, Plan *pl) {
 // by level from the top, so a leaf needs one DOWN item (its own potentials)
 // instead of one per target slot above it.  The FP64 forms keep the
 // reference's direct passes.
+// Kernel-tile store of the FP16 leaf pass: a group's stored items follow one
+// another (an item is one stage: kTcChunk sources at most), every `every`-th
+// item of the group (items every-1, 2 every-1, ...; all with every = 1).  A
+// stage of c sources holds ceil(ceil(c / 8) / 2) MMA steps of 16 sources,
+// each four chunks (hi, lo x east, north) of the group's rows rounded up to
+// 16, 32 bytes per row.
+void plan_tile_offsets(Plan *pl, int every) {
+    pl->tc_tile_off.assign(pl->tc_leaf_groups.size() + 1, 0);
+    for (size_t gi = 0; gi < pl->tc_leaf_groups.size(); ++gi) {
+        const MixGroup &m = pl->tc_leaf_groups[gi];
+        const int64_t cb = (int64_t)((m.nt + 15) & ~15) * 32;
+        int64_t b = 0;
+        for (int32_t i = m.ib; i < m.ie; ++i)
+            if ((i - m.ib) % every == every - 1) b += (int64_t)(((pl->tc_items[i].cnt + 7) / 8 + 1) / 2) * 4 * cb;
+        pl->tc_tile_off[gi + 1] = pl->tc_tile_off[gi] + b;
+    }
+}
+
 bool plan_build_tc(const Tree &t, Plan *pl, const TcOptions &opt, std::string *err) {
     const int n = t.n, np = (int)t.p.size(), d = pl->d, nd = d + 1, P = pl->P;
     const int32_t nsrc = (int32_t)pl->src_slot_panel.size(), ntgt = (int32_t)pl->tgt_slot_panel.size();
@@ -685,19 +703,7 @@ bool plan_build_tc(const Tree &t, Plan *pl, const TcOptions &opt, std::string *e
         }
     }
     if (!tree) pl->tc_macs_down = pl->macs_down;
-    // Kernel-tile store of the FP16 leaf pass: a group's tiles follow its
-    // items (one stage each: kTcChunk sources at most); a stage of c sources
-    // holds ceil(ceil(c / 8) / 2) MMA steps of 16 sources, each four chunks
-    // (hi, lo x east, north) of the group's rows rounded up to 16, 32 bytes
-    // per row.
-    pl->tc_tile_off.assign(pl->tc_leaf_groups.size() + 1, 0);
-    for (size_t gi = 0; gi < pl->tc_leaf_groups.size(); ++gi) {
-        const MixGroup &m = pl->tc_leaf_groups[gi];
-        const int64_t cb = (int64_t)((m.nt + 15) & ~15) * 32;
-        int64_t b = 0;
-        for (int32_t i = m.ib; i < m.ie; ++i) b += (int64_t)(((pl->tc_items[i].cnt + 7) / 8 + 1) / 2) * 4 * cb;
-        pl->tc_tile_off[gi + 1] = pl->tc_tile_off[gi] + b;
-    }
+    plan_tile_offsets(pl, opt.tile_store > 1 ? opt.tile_store : 1);
 
     // ---- proxy pass: each target slot's items cut into units of at most
     // proxy_unit_kpairs * 1024 pairs; rows of at most kTcProxyRows proxies

@@ -117,8 +117,9 @@ struct TcOptions {
     int32_t f16 = 0;                    // leaf pass: 1: FP16 hi/lo operands (kind::f16, 16 sources per MMA)
                                         //    with power-of-two scales; 0: TF32 hi/lo (8 sources per MMA)
     int32_t tile_store = 0;             // FP16 leaf pass: 1: its kernel tiles are kept in device memory
-                                        //    (recorded by the first solve, replayed after); the plan is the
-                                        //    same either way
+                                        //    (recorded by the first solve, replayed after); m > 1: one item in
+                                        //    m is kept and replayed, the producers compute the others; the
+                                        //    plan is the same either way
 };
 
 struct Plan {
@@ -153,8 +154,9 @@ struct Plan {
     // if >= 0, phiF row -2-v if <= -2, zero row if -1; every leaf, source
     // slot and target slot starts on a multiple of 8 rows).
     std::vector<MixGroup> tc_leaf_groups;
-    // FP16 kernel-tile store: per leaf group the byte offset of its tiles
-    // (ngroups + 1 entries; the last is the store's size)
+    // FP16 kernel-tile store: per leaf group the byte offset of its stored
+    // tiles (ngroups + 1 entries; the last is the store's size), for the
+    // current sal_tune.tile_store (plan_tile_offsets)
     std::vector<int64_t> tc_tile_off;
     std::vector<TcItem> tc_items;
     // tcgen05 proxy pass: per proxy unit, row chunks of at most kTcProxyRows
@@ -208,6 +210,8 @@ bool plan_build(const Tree &t, int d, int mode, const int32_t *list, int64_t nli
                 const int32_t *pp, int64_t npp, Plan *plan, std::string *err);
 // (Re)builds the tcgen05 part of a DTT plan for the given options.
 bool plan_build_tc(const Tree &t, Plan *plan, const TcOptions &opt, std::string *err);
+// the kernel-tile store's per-group offsets for one stored item in `every`
+void plan_tile_offsets(Plan *plan, int every);
 // The 32-field (mma.sync) groups of the batched form, from a built plan.
 void plan_build_mix(const Tree &t, Plan *plan);
 

@@ -666,7 +666,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(const __grid_const
             // rounded up to 16, each the bytes of the ring's rows
             const int nr16 = (G.nt + 15) & ~15;
             const size_t cb = (size_t)nr16 * 32;
-            unsigned char *gtile = TS == 1 ? a.ktile + a.ktile_off[gi - J.beg[gk]] : nullptr;
+            unsigned char *gtile = (TS == 1 || TS == 3) ? a.ktile + a.ktile_off[gi - J.beg[gk]] : nullptr;
             // item records are read one item ahead, so their latency hides
             // behind the current item's stages
             TcItem nxt = a.items[G.ib];
@@ -675,6 +675,30 @@ __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(const __grid_const
                 if (k + 1 < ni) nxt = a.items[G.ib + k + 1];
                 const int kind = it.kind & 3;
                 const int nst = (it.cnt + SK - 1) / SK;
+                // an item the kernel-tile store holds (one in tile_every)
+                const bool stored = (TS == 1 || TS == 3) && k % a.tile_every == a.tile_every - 1;
+                if (TS == 3 && stored) {
+                    // replay: warp 0 copies the stage's chunks (MMA step q / 4, hi / lo,
+                    // east / north) into the ring slot once the MMAs that last read it
+                    // are done; its arrival carries the bytes
+                    const uint32_t slot = st % KS, kpar = ((st / KS) - 1) & 1;
+                    const int nq = 4 * (((min(SK, it.cnt) + 7) / 8 + 1) / 2);
+                    if (st >= (uint32_t)KS) wait_bounded(&sm.kempty[slot], kpar, abort, err);
+                    if (warp == 0) {
+                        if (lane == 0) dev::mbar_expect_tx(&sm.kfull[slot], (uint32_t)(nq * cb));
+                        __syncwarp();
+                        if (lane < nq && !*abort)
+                            dev::bulk_g2s_hint(reinterpret_cast<unsigned char *>(sm.Kt(slot, lane >> 2, (lane >> 1) & 1)) +
+                                                   (lane & 1) * (kTcRows / 8) * 256,
+                                               gtile + (size_t)lane * cb, (uint32_t)cb, &sm.kfull[slot], dev::l2_evict_first());
+                    } else if (lane == 0) {
+                        mbar_arrive(&sm.kfull[slot]);
+                    }
+                    __syncwarp();
+                    gtile += (size_t)nq * cb;
+                    ++st;
+                    continue;
+                }
                 if (MODE == 0 && kind == 2 && it.off != cur_slot) {
                     // BLI bases of every target row in the new slot: thread
                     // t < 128 the xi basis of target t, thread 128 + t its
@@ -809,7 +833,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(const __grid_const
                                 *reinterpret_cast<uint4 *>(tlo + oe16 + hb) = el;
                                 *reinterpret_cast<uint4 *>(th + on16 + hb) = nh;
                                 *reinterpret_cast<uint4 *>(tlo + on16 + hb) = nl;
-                                if (TS == 1 && row < nr16) {
+                                if (TS == 1 && stored && row < nr16) {
                                     unsigned char *g = gtile + (size_t)(kk >> 1) * 4 * cb + oe16 + hb;
                                     *reinterpret_cast<uint4 *>(g) = eh;
                                     *reinterpret_cast<uint4 *>(g + cb) = nh;
@@ -889,7 +913,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(const __grid_const
                     }
                     __syncwarp();
                     if (lane == 0) mbar_arrive(&sm.kfull[slot]);
-                    if (TS == 1) gtile += (size_t)4 * ((nks + 1) >> 1) * cb;
+                    if (TS == 1 && stored) gtile += (size_t)4 * ((nks + 1) >> 1) * cb;
                 }
             }
         }
@@ -1405,6 +1429,8 @@ void launch_tc_leaf(const TcArgs &a, int nsm, int cg, int *err, cudaStream_t st,
         launch_tc<0, true, 1>(a, nsm, cg, err, st);
     else if (a.bstore16 && a.ktile && tiles == 2)
         launch_tc<0, true, 2>(a, nsm, cg, err, st);
+    else if (a.bstore16 && a.ktile && tiles == 3)
+        launch_tc<0, true, 3>(a, nsm, cg, err, st);
     else if (a.bstore16)
         launch_tc<0, true>(a, nsm, cg, err, st);
     else

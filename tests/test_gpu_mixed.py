@@ -356,11 +356,12 @@ def test_f16_batch_invariance_and_zero_field():
         assert torch.equal(ox[0], bx[f]) and torch.equal(oy[0], by[f])
 
 
-@pytest.mark.parametrize("degree,tree", [(8, 1), (8, 0), (10, 1)])
-def test_tile_store_records_and_replays_bitwise(degree, tree):
+@pytest.mark.parametrize("degree,tree,every", [(8, 1, 1), (8, 0, 1), (10, 1, 1), (8, 1, 2), (8, 0, 3)])
+def test_tile_store_records_and_replays_bitwise(degree, tree, every):
     """sal_tune.tile_store = 1: the first FP16 leaf pass records its kernel
     tiles (near-field, proxy and DOWN rows) in device memory and later solves
-    replay them.  The recording solve, the replays (other fields, fewer fields,
+    replay them; tile_store = m > 1 keeps one item in m of each group, which
+    later solves copy while the producers compute the others.  The recording solve, the replays (other fields, fewer fields,
     graphs on a stream) and the solve after switching the store off again all
     equal the computing leaf pass bit for bit; the memory estimate counts the
     store, whose size the stats report."""
@@ -372,10 +373,11 @@ def test_tile_store_records_and_replays_bitwise(degree, tree):
     ref = [v.clone() for v in grid.solve(ssh, form=S.FORM_MIXED)]
     ref3 = [v.clone() for v in grid.solve(ssh[2:5], form=S.FORM_MIXED)]
     torch.cuda.synchronize()
+    full_bytes = grid.stats()["tile_store_bytes"]
+    grid.tune(tile_store=every)
+    assert grid.tune()["tile_store"] == every
     tile_bytes = grid.stats()["tile_store_bytes"]
-    assert tile_bytes > 0
-    grid.tune(tile_store=1)
-    assert grid.tune()["tile_store"] == 1
+    assert 0 < tile_bytes <= full_bytes and (every == 1) == (tile_bytes == full_bytes)
     est = grid.stats()["mixed_bytes"]
     before = grid.stats()["device_bytes"]
     for k in range(3):   # record, then replays
