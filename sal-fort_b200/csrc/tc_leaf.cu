@@ -347,118 +347,132 @@ __device__ __forceinline__ void emit_chunk(const float (&x)[16], int c0, int f, 
     }
 }
 
-// Folds a finished accumulator chain (warp-collective; this warp's lane
-// quarter q: fields 16q..16q+15, hi rows in lanes 0-15 and lo rows in lanes
-// 16-31, for the group's 256 columns).  The running sums live in tensor
-// memory next to the accumulator (columns 256-511, same row layout), hi and
-// lo rows apart: mid-group, running sum (+)= chain with round-to-nearest FP32
-// adds (the group's first chain stores); at the group's end, running sum +
-// chain goes to the caller's outputs, hi + lo added in FP64.
+// Folds a finished accumulator chain into the running sums (warp-collective;
+// this warp's lane quarter q: fields 16q..16q+15, hi rows in lanes 0-15 and
+// lo rows in lanes 16-31).  The running sums live in tensor memory next to
+// the accumulator (columns 256-511, same row layout): running sum (+)= chain
+// with round-to-nearest FP32 adds (the group's first chain stores).  At a
+// group's end only the chunks that hold targets are folded, and emit_sums
+// writes them out after the accumulator has been handed back to the MMA
+// warp, so the next group's first chain overlaps the output writes.
 // MODE 0 (leaf): columns half c + t are component c (east, north) of target
 // t (half = 128, or the group's rows rounded up to 16 for the packed tiles of
-// a replayed kernel-tile store), ends go to the caller's outputs.  MODE 1 (proxy): columns 85c + r are
-// Cartesian component c of proxy r, ends go to the unit's partial rows `part`.
-// MODE 2 (upward): columns j < 128 are proxies row0 + j.
+// a replayed kernel-tile store).  MODE 1 (proxy): columns 85c + r are
+// Cartesian component c of proxy r.  MODE 2 (upward): columns j < 128 are
+// proxies row0 + j.
 //
 // FP16 leaf pass (scaled, the same in every lane): the chain's operands were
 // scaled by powers of two, the weight rows of field f by 1 / fsc and (kernel
 // chains) the kernel tile's column of target t by tscale[tgt + t] (DOWN
 // chains: unscaled columns).  The running sums are kept in the columns'
 // scaled domain: a kernel chain adds chain x fsc, a DOWN chain chain x fsc x
-// tscale, and the group's end multiplies by tinv = 1 / tscale.  Powers of two
+// tscale, and emit_sums multiplies by tinv = 1 / tscale.  Powers of two
 // commute with rounding, so this gives the unscaled sums' bits while kernel
 // chains (all but one or a few per group) need no per-column factors.
 // Several warps of one lane quarter can share a fold: warp part_i of nparts
-// takes chunks part_i, part_i + nparts, ... (pairs of chunks mid-group).
+// takes the chunk pairs (2p, 2p + 1) with p % nparts == part_i, and emits
+// the same chunks.
+
+// Chunks of 16 columns a fold covers: per component, at a group's end only
+// those that hold targets; a pair (2p, 2p + 1) at a time.
 template <int MODE>
-__device__ __noinline__ void fold_chain(uint32_t td, int q, int lane, bool end, bool first, int tgt, int nt,
-                                        const int32_t *__restrict__ perm, double *out_x, double *out_y,
-                                        int64_t ld_out, int f0, int nf, bool skip, float *part, bool scaled = false,
-                                        float fsc = 1.f, bool down = false, const float *__restrict__ tscale = nullptr,
-                                        const float *__restrict__ tinv = nullptr, int half = 128, int part_i = 0,
-                                        int nparts = 1) {
-    const int f = 16 * q + (lane & 15), odd = lane >> 4;
-    // per target slot 32k + lane: its scale (DOWN chains) and inverse (the end)
-    float csd[4] = {1.f, 1.f, 1.f, 1.f}, cse[4] = {1.f, 1.f, 1.f, 1.f};
+__device__ __forceinline__ int fold_per(bool end, int nt, int half) {
+    return (MODE != 1 && end) ? (nt + 15) / 16 : (MODE == 0 ? half / 16 : 8);
+}
+
+template <int MODE>
+__device__ __noinline__ void fold_chain(uint32_t td, int lane, bool end, bool first, int tgt, int nt, bool scaled,
+                                        float fsc, bool down, const float *__restrict__ tscale, int half, int part_i,
+                                        int nparts) {
+    // per target slot 32k + lane: its scale (DOWN chains)
+    float csd[4] = {1.f, 1.f, 1.f, 1.f};
     if (MODE == 0 && scaled && down)
 #pragma unroll
         for (int k = 0; k < 4; ++k) csd[k] = 32 * k + lane < nt ? tscale[tgt + 32 * k + lane] : 1.f;
-    if (MODE == 0 && scaled && end)
-#pragma unroll
-        for (int k = 0; k < 4; ++k) cse[k] = 32 * k + lane < nt ? tinv[tgt + 32 * k + lane] : 1.f;
-    // x[m] *= v[column c + m] for a 16-column chunk starting at column c
-    auto colmul = [&](float (&x)[16], int c, const float (&v)[4]) {
-        const int b = c >= half ? c - half : c, k = b >> 5;
-        const float src = k == 0 ? v[0] : k == 1 ? v[1] : k == 2 ? v[2] : v[3];
-#pragma unroll
-        for (int m = 0; m < 16; ++m) x[m] *= __shfl_sync(0xffffffffu, src, (b & 31) + m);
-    };
-    // the chain into the running sums' domain
+    // the chain into the running sums' domain, on a 16-column chunk starting at column c
     auto unscale = [&](float (&x)[16], int c) {
         if (!scaled) return;
 #pragma unroll
         for (int m = 0; m < 16; ++m) x[m] *= fsc;
-        if (down) colmul(x, c, csd);
-    };
-    int idx[4] = {0, 0, 0, 0};   // caller index of target slot 32k + lane
-    if (MODE == 0 && end)
+        if (down) {
+            const int b = c >= half ? c - half : c, k = b >> 5;
+            const float src = k == 0 ? csd[0] : k == 1 ? csd[1] : k == 2 ? csd[2] : csd[3];
 #pragma unroll
-        for (int k = 0; k < 4; ++k) idx[k] = 32 * k + lane < nt ? perm[tgt + 32 * k + lane] : 0;
-    const bool wr = end && (MODE != 0 || f0 + f < nf) && !skip;
-    double *ox = MODE == 0 ? out_x + (size_t)(f0 + f) * ld_out : nullptr;
-    double *oy = MODE == 0 ? out_y + (size_t)(f0 + f) * ld_out : nullptr;
-    // chunks of 16 columns: leaf component ch = c / half, target slots
-    // c % half ..+15 (at a group's end only the chunks that hold targets);
-    // proxy: all 16 chunks
-    const int per = (MODE != 1 && end) ? (nt + 15) / 16 : (MODE == 0 ? half / 16 : 8);
+            for (int m = 0; m < 16; ++m) x[m] *= __shfl_sync(0xffffffffu, src, (b & 31) + m);
+        }
+    };
+    const int per = fold_per<MODE>(end, nt, half);
     const int nchunk = MODE == 2 ? per : 2 * per;   // upward: one component, columns 0..127
     auto col = [&](int i) { return (i / per) * half + (i % per) * 16; };
-    if (!end) {
-        // mid-group: the MMA warp waits for this fold before its next chain,
-        // so two chunks' loads are in flight per wait (nchunk is even here)
-        float x0[16], x1[16], r0[16], r1[16];
+    // two chunks' loads in flight per wait: the MMA warp waits for this fold
+    float x0[16], x1[16], r0[16], r1[16];
 #pragma unroll 1
-        for (int i = 2 * part_i; i < nchunk; i += 2 * nparts) {
-            const int c0 = col(i), c1 = col(i + 1);
-            tmem_ld16(td + c0, x0);
-            tmem_ld16(td + c1, x1);
-            if (!first) {
-                tmem_ld16(td + 256 + c0, r0);
-                tmem_ld16(td + 256 + c1, r1);
-            }
-            tmem_wait_ld();
-            unscale(x0, c0);
-            unscale(x1, c1);
-            if (!first) {
-#pragma unroll
-                for (int m = 0; m < 16; ++m) {
-                    x0[m] += r0[m];
-                    x1[m] += r1[m];
-                }
-            }
-            tmem_st16(td + 256 + c0, x0);
-            tmem_st16(td + 256 + c1, x1);
+    for (int i = 2 * part_i; i < nchunk; i += 2 * nparts) {
+        const bool two = i + 1 < nchunk;   // a group's end in the upward pass can leave one
+        const int c0 = col(i), c1 = col(two ? i + 1 : i);
+        tmem_ld16(td + c0, x0);
+        tmem_ld16(td + c1, x1);
+        if (!first) {
+            tmem_ld16(td + 256 + c0, r0);
+            tmem_ld16(td + 256 + c1, r1);
         }
-        tmem_wait_st();
-        return;
-    }
-    float x[16], r[16];
-#pragma unroll 1
-    for (int i = part_i; i < nchunk; i += nparts) {
-        const int c = col(i);
-        tmem_ld16(td + c, x);
-        if (!first) tmem_ld16(td + 256 + c, r);
         tmem_wait_ld();
-        unscale(x, c);
+        unscale(x0, c0);
+        unscale(x1, c1);
         if (!first) {
 #pragma unroll
-            for (int m = 0; m < 16; ++m) x[m] += r[m];
+            for (int m = 0; m < 16; ++m) {
+                x0[m] += r0[m];
+                x1[m] += r1[m];
+            }
         }
-        if (MODE == 0 && scaled) colmul(x, c, cse);   // out of the columns' scaled domain
-        const int ik = (c >= half ? c - half : c) >> 5;
-        const int idk = ik == 0 ? idx[0] : ik == 1 ? idx[1] : ik == 2 ? idx[2] : idx[3];
-        emit_chunk<MODE>(x, c, f, odd, nt, idk, c < half ? ox : oy, wr, part, half);
+        tmem_st16(td + 256 + c0, x0);
+        if (two) tmem_st16(td + 256 + c1, x1);
     }
+    tmem_wait_st();
+}
+
+// A group's end: its running sums (this warp's chunks of fold_chain) to the
+// destinations, hi + lo added in FP64: MODE 0 the caller's outputs, MODE 1 /
+// 2 the unit's partial rows `part`.
+template <int MODE>
+__device__ __noinline__ void emit_sums(uint32_t td, int q, int lane, int tgt, int nt, const int32_t *__restrict__ perm,
+                                       double *out_x, double *out_y, int64_t ld_out, int f0, int nf, bool skip,
+                                       float *part, bool scaled, const float *__restrict__ tinv, int half, int part_i,
+                                       int nparts) {
+    const int f = 16 * q + (lane & 15), odd = lane >> 4;
+    float cse[4] = {1.f, 1.f, 1.f, 1.f};   // per target slot 32k + lane: its scale's inverse
+    if (MODE == 0 && scaled)
+#pragma unroll
+        for (int k = 0; k < 4; ++k) cse[k] = 32 * k + lane < nt ? tinv[tgt + 32 * k + lane] : 1.f;
+    int idx[4] = {0, 0, 0, 0};   // caller index of target slot 32k + lane
+    if (MODE == 0)
+#pragma unroll
+        for (int k = 0; k < 4; ++k) idx[k] = 32 * k + lane < nt ? perm[tgt + 32 * k + lane] : 0;
+    const bool wr = (MODE != 0 || f0 + f < nf) && !skip;
+    double *ox = MODE == 0 ? out_x + (size_t)(f0 + f) * ld_out : nullptr;
+    double *oy = MODE == 0 ? out_y + (size_t)(f0 + f) * ld_out : nullptr;
+    const int per = fold_per<MODE>(true, nt, half);
+    const int nchunk = MODE == 2 ? per : 2 * per;
+    auto col = [&](int i) { return (i / per) * half + (i % per) * 16; };
+    float x[16];
+#pragma unroll 1
+    for (int i = 2 * part_i; i < nchunk; i += 2 * nparts)
+#pragma unroll 1
+        for (int h = i; h < i + 2 && h < nchunk; ++h) {
+            const int c = col(h);
+            tmem_ld16(td + 256 + c, x);
+            tmem_wait_ld();
+            const int b = c >= half ? c - half : c, k = b >> 5;
+            if (MODE == 0 && scaled) {
+                // out of the columns' scaled domain
+                const float src = k == 0 ? cse[0] : k == 1 ? cse[1] : k == 2 ? cse[2] : cse[3];
+#pragma unroll
+                for (int m = 0; m < 16; ++m) x[m] *= __shfl_sync(0xffffffffu, src, (b & 31) + m);
+            }
+            const int idk = k == 0 ? idx[0] : k == 1 ? idx[1] : k == 2 ? idx[2] : idx[3];
+            emit_chunk<MODE>(x, c, f, odd, nt, idk, c < half ? ox : oy, wr, part, half);
+        }
 }
 
 // Outputs of target t of a leaf group without sources: its self pair alone.
@@ -1126,6 +1140,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(const __grid_const
                 continue;
             }
             bool first = true;
+            const int half = TS == 2 ? (G.nt + 15) & ~15 : 128;   // columns per component
             ItemWindow w;
             w.start(a.items, G.ib, G.ie, lane);
             for (int k = G.ib; k < G.ie; ++k) {
@@ -1139,16 +1154,20 @@ __global__ void __launch_bounds__(kThreads, 1) tc_leaf_kernel(const __grid_const
                 const bool down_chain = (kind & 3) == 2;
                 const float fsc = F16 ? 1.f / f16_scale(__uint_as_float(a.fmax[(down_chain ? kF : 0) + 16 * q + (lane & 15)]))
                                       : 1.f;
-                fold_chain<MODE>(tq, q, lane, k == G.ie - 1, first, G.tgt, G.nt,
-                                 a.perm, a.out_x, a.out_y, a.ld_out, a.f0, a.nf, *abort != 0,
-                                 MODE == 1   ? a.partial + ((size_t)G.out * P + G.row0) * 3 * kF
-                                 : MODE == 2 ? a.partial + ((size_t)G.out * P + G.row0) * kF
-                                             : nullptr,
-                                 F16, fsc, down_chain, a.tscale, a.tinv, TS == 2 ? (G.nt + 15) & ~15 : 128, part_i,
+                const bool end = k == G.ie - 1;
+                fold_chain<MODE>(tq, lane, end, first, G.tgt, G.nt, F16, fsc, down_chain, a.tscale, half, part_i,
                                  nparts);
                 tc_fence_before();
                 __syncwarp();
                 if (lane == 0) mbar_arrive(&sm.accfree);
+                // the next group's first chain may run into the accumulator meanwhile
+                if (end)
+                    emit_sums<MODE>(tq, q, lane, G.tgt, G.nt, a.perm, a.out_x, a.out_y, a.ld_out, a.f0, a.nf,
+                                    *abort != 0,
+                                    MODE == 1   ? a.partial + ((size_t)G.out * P + G.row0) * 3 * kF
+                                    : MODE == 2 ? a.partial + ((size_t)G.out * P + G.row0) * kF
+                                                : nullptr,
+                                    F16, a.tinv, half, part_i, nparts);
                 first = false;
                 ++cc;
             }
