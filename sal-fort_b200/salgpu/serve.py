@@ -201,6 +201,16 @@ class Server:
             g.set_graphs(True)
         self._alloc_staging(r)
 
+    def reserve(self, nbytes: int) -> None:
+        """Grows torch's caching allocator on the serving device by nbytes
+        (one block, freed at once and kept in the cache): requests' fields and
+        results are then carved from it instead of cudaMalloc calls in the
+        middle of the request stream."""
+        if self.torch is None or nbytes <= 0:
+            return
+        blk = self.torch.empty(int(nbytes), dtype=self.torch.uint8, device=self.torch.device("cuda", self.device))
+        del blk
+
     # ------------------------------------------------------------------ device hooks
     # (a test double overrides these four to exercise the scheduling on the CPU)
     def _stream_priority(self, r: _Resident) -> int:
