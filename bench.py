@@ -438,10 +438,12 @@ def serving_run(args, S, torch, dev):
     # requests in flight at once hold fields and results of up to a few GB:
     # the allocator's cache holds that much before the clock starts
     srv.reserve(12 << 30)
+    srv.slowest.clear()
     t0 = time.perf_counter()
     reqs = serve.run_workload(srv, pools, weights, args.serve_rate, args.serve_seconds, seed=7, keep=2)
     wall = time.perf_counter() - t0
     out = serve.summarize(reqs, sizes, wall, srv.batches)
+    out["slowest_host_calls_ms"] = {k: round(v * 1e3, 2) for k, v in sorted(srv.slowest.items(), key=lambda kv: -kv[1])[:6]}
     out.update({"rate_req_per_s": args.serve_rate, "seconds": args.serve_seconds, "max_batch_fields": 64,
                 "evictions": srv.evictions, "requests_on": "host" if args.serve_host else "device"})
     # accuracy of served results: first field of a few requests of each grid

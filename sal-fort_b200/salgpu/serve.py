@@ -147,6 +147,7 @@ class Server:
         # CTAs short, so higher-priority grids' kernels get SMs quickly
         self.tune = dict(f16=1, chain_ksteps=64) if tune is None else dict(tune)
         self.batches: list[tuple] = []     # (grid, fields, launch time, done time) of finished batches
+        self.slowest: dict = {}            # the longest host-side launch / poll / results call per grid, seconds
 
     # ------------------------------------------------------------------ grids
     def register_grid(self, spec: GridSpec) -> None:
@@ -333,13 +334,23 @@ class Server:
                 return
         for q in batch:
             q.status = "running"
+        t0 = self.clock()
         self._launch_device(r, batch, nf)
+        self._note_slow("launch " + r.spec.name, self.clock() - t0)
         r.inflight = batch
         r.last_used = r.launched = self.clock()
         self.grids.move_to_end(r.spec.name)
 
+    def _note_slow(self, what: str, dt: float) -> None:
+        # the slowest host-side step of each kind: where a stalled loop spends its time
+        if dt > self.slowest.get(what, 0.0):
+            self.slowest[what] = dt
+
     def _reap(self, r: _Resident) -> None:
-        if r.inflight is None or not self._batch_done(r):
+        t0 = self.clock()
+        done = r.inflight is not None and self._batch_done(r)
+        self._note_slow("poll " + r.spec.name, self.clock() - t0)
+        if not done:
             return
         now = self.clock()
         f = 0
@@ -355,6 +366,7 @@ class Server:
             q.done_time = now
             f += q.nfields
             self.completed.append(q)
+        self._note_slow("results " + r.spec.name, self.clock() - now)
         self.batches.append((r.spec.name, f, r.launched, now))
         dt = now - r.launched
         r.batch_time = dt if r.batch_time == 0.0 else 0.8 * r.batch_time + 0.2 * dt
