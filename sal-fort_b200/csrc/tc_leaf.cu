@@ -46,6 +46,14 @@
 // source weights and its potentials by powers of two of their own (per
 // solve), and the fold divides them out of each chain; DOWN items (O(1)
 // interpolation weights against potentials) form chains of their own.
+// Kernel-tile store (sal_tune.tile_store, FP16 leaf pass): the kernel tiles
+// depend on the grid alone.  A recording launch (TS 1) computes them and also
+// writes them to device memory; a replaying launch (TS 2) has the loader copy
+// each stage's tiles and weights into two shared-memory byte rings, and the
+// idle producer warps fold beside the fold warps; a partial replay (TS 3)
+// has producer warp 0 copy the stored items' tiles into the ring slot while
+// the producers compute the others.  All three give the computing launch's
+// results bit for bit.
 // The tensor cores accumulate with truncation, so one chain over all of a
 // target's sources would bias the result toward zero: a chain ends after about
 // 32 k-steps (plan flag kTcFlush) and is folded into the group's running sums
