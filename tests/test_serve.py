@@ -81,6 +81,24 @@ def test_batching_packs_whole_requests_fifo():
     assert all(q.status == "done" for q in reqs)
 
 
+def test_summary_reports_launch_gaps_and_slowest_host_calls():
+    """The serving summary's diagnostics: per grid the longest batch, the
+    longest stretch with no batch launched, and the loop's slowest host calls
+    (launch, poll, results) per grid."""
+    from salgpu import serve
+    srv = _fake_server(10 ** 9, max_batch=8)
+    srv.register_grid(_spec("a", 300))
+    reqs = [srv.submit(serve.Request("a", np.zeros((5, 300)))) for _ in range(3)]
+    srv.run_until_idle(poll_s=0)
+    assert len(srv.batches) == 3                      # 5 + 5 fields do not fit a batch of 8
+    out = serve.summarize(reqs, {"a": 300}, 1.0, srv.batches)
+    launches = sorted(b[2] for b in srv.batches)
+    assert out["max_launch_gap_ms"] == pytest.approx(1e3 * float(np.max(np.diff(launches))))
+    assert out["per_grid"]["a"]["max_batch_ms"] == pytest.approx(1e3 * max(b[3] - b[2] for b in srv.batches))
+    assert {"launch a", "poll a", "results a"} <= set(srv.slowest)
+    assert all(v > 0 for v in srv.slowest.values())
+
+
 def test_admission_evicts_least_recently_used_idle_grid():
     from salgpu import serve
     budget = _bytes(400) + _bytes(500) + 10          # two of the three grids fit
